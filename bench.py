@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark of the radix-partitioned inner equi-join on B200.
+
+Workload (one "step"): the 2^27 x 2^27 int32 join -- build keys a seeded
+permutation of 1..2^27, probe keys 90 % uniform from the build keys and 10 %
+outside [1, 2^27] -- run once through the C ABI (pj_inner_join), inputs
+resident in HBM.  Inputs (1 GiB of keys) are larger than L2, so no flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU join (inner_join_cpu,
+compiled from the reference sources into oracle/_ref) on a bounded sample of
+the same workload with every host thread.  Under torchrun only rank 0 runs it.
+
+One JSON line on rank 0.  value = input tuples / s over all ranks (each rank
+joins its own replica of the workload: weak scaling, no data-path
+collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "tuples/s & HBM-roofline %, 2^27x2^27 int32 join"
+UNIT = "tuples/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log2-build", type=int, default=27)
+    ap.add_argument("--log2-probe", type=int, default=27)
+    ap.add_argument("--match-rate", type=float, default=0.9)
+    ap.add_argument("--cpu-sample-log2", type=int, default=24,
+                    help="build and probe rows of the bounded CPU sample (log2)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plan", type=str, default="", help="JSON overrides of pj_plan fields")
+    ap.add_argument("--seed", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------------------
+# inputs
+
+def gen_config2_device(n_b, n_p, match_rate, seed, device):
+    """Seeded cfg2-shaped inputs generated on the device (torch RNG)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    build = (torch.randperm(n_b, generator=g, device=device) + 1).to(torch.int32)
+    idx = torch.randint(0, n_b, (n_p,), generator=g, device=device)
+    probe = build[idx]
+    del idx
+    miss = torch.rand(n_p, generator=g, device=device) >= match_rate
+    nm = int(miss.sum().item())
+    if nm:
+        probe[miss] = torch.randint(n_b + 1, 2**31 - 1, (nm,), generator=g, device=device).to(torch.int32)
+    expected = int((probe <= n_b).sum().item())
+    return build.contiguous(), probe.contiguous(), expected
+
+
+def cpu_sample(log2n, match_rate, seed):
+    from partitioned_join_b200 import datagen
+    n = 1 << log2n
+    return datagen.config2(seed=seed, n_build=n, n_probe=n, match_rate=match_rate)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# roofline helpers
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_tag):
+    """DRAM bytes per launch of a kernel from a committed ncu summary
+    (profiles/*.md line 'dram_bytes_per_launch[<tag>]: <bytes>'), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    pat = re.compile(r"dram_bytes_per_launch\[" + re.escape(kernel_tag) + r"\]:\s*([0-9.eE+]+)")
+    for name in sorted(os.listdir(pdir)):
+        if not name.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(pdir, name)):
+            m = pat.search(line)
+            if m:
+                return float(m.group(1))
+    return None
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference(args, rank, world):
+    """The reference's own CPU join on a bounded sample of the workload."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    b, p = cpu_sample(args.cpu_sample_log2, args.match_rate, args.seed)
+    if oracle.ref_cpu_available():
+        kind = "reference"
+        threads = oracle.ref_cpu().ref_omp_max_threads()
+        run = lambda: oracle.ref_inner_join_cpu(b, p, True)[1]  # noqa: E731
+    else:
+        kind = "port"
+        threads = 1
+
+        def run():
+            t0 = time.perf_counter()
+            oracle.inner_join(b, p, True)
+            return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        run()
+    secs = [run() for _ in range(args.steps)]
+    total = sum(secs)
+    tuples = (b.shape[0] + p.shape[0]) * args.steps
+    value = tuples / total
+    sample = (f"2^{args.cpu_sample_log2} x 2^{args.cpu_sample_log2} rows of the same generator "
+              f"(match rate {args.match_rate}); time = inner_join_cpu's own omp_get_wtime interval "
+              f"(build + probe), unique-key path")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2), "
+                               f"CPU sample 2^{args.cpu_sample_log2}x2^{args.cpu_sample_log2}",
+                   "build_rows": 1 << args.cpu_sample_log2, "probe_rows": 1 << args.cpu_sample_log2},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+
+    from partitioned_join_b200 import _lib, api
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+
+    n_b, n_p = 1 << args.log2_build, 1 << args.log2_probe
+    build, probe, expected = gen_config2_device(n_b, n_p, args.match_rate, args.seed + rank, device)
+    plan = api.plan_default(n_b, n_p, 4, True)
+    if args.plan:
+        for k, v in json.loads(args.plan).items():
+            setattr(plan, k, v)
+    j = api.Joiner(build, probe, True, plan, capacity=n_p)
+    stream = torch.cuda.current_stream()
+
+    # warm-up, and a correctness check of the count
+    for _ in range(max(args.warmup, 1)):
+        j.launch()
+    st = j.status()
+    _lib.check(st, "warm-up join")
+    got = int(j.count.item())
+    verified = got == expected
+    if not verified:
+        raise SystemExit(f"bench: join produced {got} pairs, expected {expected}")
+
+    # timed region: K steps with per-stage events
+    n_st = len(_lib.STAGES)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(n_st)] for _ in range(args.steps)]
+    for row in ev:
+        for e in row:
+            e.record(stream)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for k in range(args.steps):
+        j.launch_with_events(ev[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    _lib.check(j.status(), "timed joins")
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stage_ms = {name: 0.0 for name in _lib.STAGES[:-1]}
+    for row in ev:
+        for i, name in enumerate(_lib.STAGES[:-1]):
+            stage_ms[name] += row[i].elapsed_time(row[i + 1]) / args.steps
+    step_ms = ms / args.steps
+    tuples_all = world * (n_b + n_p) * args.steps
+    value = tuples_all / (ms / 1e3)
+
+    # roofline: the dominant kernel and the whole join
+    peak, peak_kind = measured_peak_gbs()
+    kb, tb = 4, 8  # key bytes, partitioned tuple bytes
+    alg = {
+        "build_hist": n_b * kb, "probe_hist": n_p * kb,
+        "build_scatter": n_b * (kb + tb), "probe_scatter": n_p * (kb + tb),
+        "join": (n_b + n_p) * tb + expected * 8,
+    }
+    dom = max(alg, key=lambda k: stage_ms[k])
+    achieved = alg[dom] / (stage_ms[dom] / 1e3) / 1e9
+    kernel_of = {"build_hist": "hist_keys_kernel", "probe_hist": "hist_keys_kernel",
+                 "build_scatter": "scatter_keys_kernel", "probe_scatter": "scatter_keys_kernel",
+                 "join": "join_kernel"}
+    traffic = ncu_traffic(f"{kernel_of[dom]}:{dom}")
+    b_alg = (n_b + n_p) * (4 + 4) + expected * 8          # (k+v) per input tuple + 8 per output pair
+    b_keys = (n_b + n_p) * 4 + expected * 8               # what the path must move at least
+    join_gbs = b_alg / (step_ms / 1e3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2): build = seeded "
+                               f"permutation of 1..2^{args.log2_build}, probe {args.match_rate:.0%} uniform hits",
+                   "build_rows": n_b, "probe_rows": n_p, "output_pairs": expected, "unique_build_keys": True,
+                   "l2": "inputs (1 GiB) larger than L2, no flush", "parallelism": f"replicas x{world}",
+                   "plan": plan.as_dict()},
+        "clocks": clk,
+        "gpu_launches": 9 * args.steps,
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": f"{kernel_of[dom]} ({dom})", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": alg[dom]},
+        "roofline_join": {"algorithmic_bytes": b_alg, "achieved": join_gbs, "peak": peak, "unit": "GB/s",
+                          "frac": join_gbs / peak, "frac_keys_only": (b_keys / (step_ms / 1e3) / 1e9) / peak},
+        "verified": verified,
+    }
+
+    if not args.no_e2e:
+        line["e2e"] = e2e_measure(args, j, build, probe, stream)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def e2e_measure(args, j, build, probe, stream):
+    """Host buffers in, host pairs out: H2D of both key columns from pinned
+    memory, the join through the C ABI, D2H of the count and the pairs."""
+    import torch
+    hb = build.cpu().pin_memory()
+    hp = probe.cpu().pin_memory()
+    cap = j.capacity
+    ob = torch.empty(cap, dtype=torch.int32).pin_memory()
+    op = torch.empty(cap, dtype=torch.int32).pin_memory()
+    cnt = torch.empty(1, dtype=torch.int64).pin_memory()
+    steps = max(1, min(args.steps, 5))
+    h2d = hb.numel() * 4 + hp.numel() * 4
+    d2h = []
+
+    def step():
+        j.build_keys.copy_(hb, non_blocking=True)
+        j.probe_keys.copy_(hp, non_blocking=True)
+        j.launch()
+        cnt.copy_(j.count, non_blocking=True)
+        stream.synchronize()
+        n = min(int(cnt.item()), cap)
+        ob[:n].copy_(j.build_row[:n], non_blocking=True)
+        op[:n].copy_(j.probe_row[:n], non_blocking=True)
+        stream.synchronize()
+        return 8 + 8 * n
+
+    step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        d2h.append(step())
+    secs = time.perf_counter() - t0
+    n_tuples = (j.desc.n_build + j.desc.n_probe) * steps
+    return {"value": n_tuples / secs, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": int(sum(d2h) / len(d2h)), "steps": steps,
+            "ms_per_step": 1e3 * secs / steps, "timer": "host wall clock around synchronised steps"}
+
+
+def cpu_baseline(args):
+    from oracle import oracle
+    b, p = cpu_sample(args.cpu_sample_log2, args.match_rate, args.seed)
+    if oracle.ref_cpu_available():
+        _, secs = oracle.ref_inner_join_cpu(b, p, True)
+        kind, cores = "reference", oracle.ref_cpu().ref_omp_max_threads()
+    else:
+        t0 = time.perf_counter()
+        oracle.inner_join(b, p, True)
+        secs, kind, cores = time.perf_counter() - t0, "port", 1
+    return {"value": (b.shape[0] + p.shape[0]) / secs, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"2^{args.cpu_sample_log2} x 2^{args.cpu_sample_log2} rows of the cfg2 generator, "
+                      f"inner_join_cpu's own timer (build + probe)"}
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

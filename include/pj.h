@@ -1,0 +1,232 @@
+/*
+ * pj.h -- C ABI of the B200-native radix-partitioned inner equi-join.
+ *
+ * Replaces the reference's `partitioned_join` stage sequence
+ * (main.cu:762-892), whose stages are header templates called with raw
+ * device pointers:
+ *   partition_input_tables_pass_one   src/partitioned_join.cuh:51-107
+ *   partition_input_tables_pass_two   src/partitioned_join.cuh:110-175
+ *   combined_histogram_pass           src/partitioned_join.cuh:22-48
+ *   handle_skewed_data                src/skewed_data_handler.cuh:59-91
+ *   shared_memory_hash_join           src/partitioned_join.cuh:178-251
+ *   inner_join_cpu (output contract)  src/inner_join_cpu.hpp:24-107
+ *
+ * Conventions
+ *  - Every pointer in a descriptor is a DEVICE pointer unless stated.
+ *  - Keys are signed 4- or 8-byte integers (the reference's key_type,
+ *    common.cuh:25-39, chosen at run time instead of by -DUSE_8B_KEYS).
+ *    Every key value joins, including -1 (the reference's empty-slot
+ *    sentinel, hash_join_kernels.cuh:20, which it cannot join).
+ *  - Output is a pair of int32 row-index columns (build_row, probe_row), one
+ *    entry per matching (build, probe) pair, in no particular order.
+ *  - The library never allocates device memory: callers size a workspace
+ *    with pj_workspace_size() and pass it in.  Inputs are never modified
+ *    (the reference overwrites its inputs in two-pass mode, main.cu:833-838).
+ *  - Calls are asynchronous on the given stream (a cudaStream_t; NULL is the
+ *    legacy default stream) unless documented as synchronising.  Argument
+ *    errors are returned at once; device-side conditions (output capacity,
+ *    table overflow, bounded-wait timeout) are recorded in the workspace and
+ *    returned by pj_check() after the stream work completes.
+ *  - Distinct workspaces may be used concurrently from different threads.
+ */
+#ifndef PJ_H
+#define PJ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pj_status {
+    PJ_OK = 0,
+    PJ_ERR_INVALID = 1,     /* bad argument or unsupported combination */
+    PJ_ERR_CAPACITY = 2,    /* output capacity too small; *count holds the required count */
+    PJ_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    PJ_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    PJ_ERR_WORKSPACE = 5,   /* workspace missing, misaligned or too small */
+    PJ_ERR_OVERFLOW = 6,    /* a shared-memory table overflowed: the plan was too coarse */
+    PJ_ERR_ALIGNMENT = 7,   /* an input column is not 16-byte aligned */
+    PJ_ERR_INTERNAL = 8     /* a device-side consistency check failed */
+} pj_status;
+
+/* cudaStream_t, kept opaque so that this header needs no CUDA headers. */
+typedef void* pj_stream;
+
+/* Digit source for radix partitioning. */
+enum {
+    PJ_DIGIT_RAW = 0,  /* raw key bits, as the reference: partition_kernels.cuh:168,380 */
+    PJ_DIGIT_HASH = 1  /* top bits of MurmurHash3_32(key): robust to key patterns */
+};
+
+/* Slot function inside a partition's shared-memory table. */
+enum {
+    PJ_SLOT_FAST = 0,  /* multiply-high range reduction of the unused hash bits */
+    PJ_SLOT_REF = 1    /* abs((int)hash % T), as the reference: hash_join_kernels.cuh:100-101 */
+};
+
+/* How a partition whose build side exceeds one table is split over CTAs. */
+enum {
+    PJ_SPLIT_HASH = 0,     /* by hash bits: each probe row visits one table */
+    PJ_SPLIT_POSITION = 1  /* by build-row position, every chunk probes all rows:
+                              the reference's skew split, skewed_data_handler.cuh:21-43 */
+};
+
+/* One join: build and probe key columns (and optional payload columns). */
+typedef struct pj_join_desc {
+    const void* build_keys;     /* n_build keys of key_bytes each, 16-byte aligned */
+    const void* probe_keys;     /* n_probe keys, 16-byte aligned */
+    const void* build_payload;  /* optional (NULL): gathered into pj_output.build_payload_out */
+    const void* probe_payload;  /* optional (NULL) */
+    int64_t n_build;            /* 0 .. 2^31-1 */
+    int64_t n_probe;            /* 0 .. 2^31-1 */
+    int32_t key_bytes;          /* 4 or 8 */
+    int32_t payload_bytes;      /* 0, 4 or 8 */
+    int32_t unique_build_keys;  /* non-zero: each probe row matches at most one build row
+                                   (the reference's -u, inner_join_cpu.hpp:41-78) */
+    int32_t reserved;
+} pj_join_desc;
+
+/* Caller-allocated device output. */
+typedef struct pj_output {
+    int32_t* build_row;         /* capacity entries */
+    int32_t* probe_row;         /* capacity entries */
+    int64_t capacity;
+    int64_t* count;             /* device int64: number of matches (may exceed capacity) */
+    void* build_payload_out;    /* optional: build_payload[build_row[i]] */
+    void* probe_payload_out;    /* optional: probe_payload[probe_row[i]] */
+} pj_output;
+
+/* Execution plan.  pj_plan_default() fills it from the sizes alone,
+ * pj_plan_exact() from an exact device histogram.  Passing NULL to
+ * pj_inner_join() uses pj_plan_default(). */
+typedef struct pj_plan {
+    int32_t passes;             /* 1 or 2 radix passes */
+    int32_t bits1;              /* radix bits of pass 1 */
+    int32_t bits2;              /* radix bits of pass 2 (0 when passes == 1) */
+    int32_t digit_mode;         /* PJ_DIGIT_* */
+    int32_t slot_mode;          /* PJ_SLOT_* */
+    int32_t split_mode;         /* PJ_SPLIT_* */
+    int32_t table_slots;        /* slots of one shared-memory table */
+    int32_t probe_chunk;        /* probe rows of one join work item */
+    int32_t join_threads;       /* threads per join CTA */
+    int32_t scatter_threads;    /* threads per scatter CTA */
+    int32_t scatter_ctas_per_sm;/* resident scatter CTAs per SM (its chunks) */
+    int32_t flags;              /* reserved, 0 */
+    float max_fill;             /* target table fill (the reference's HASH_TABLE_OCC = 0.5) */
+    float reserved_f;
+} pj_plan;
+
+/* Human-readable text of a status. */
+const char* pj_status_string(pj_status s);
+
+/* Library version string. */
+const char* pj_version(void);
+
+/* Plan from the sizes alone (no device work, no synchronisation).  Mirrors
+ * the reference's static choice of -n/-N/-f (main.cu:239-251,867) with
+ * B200 shared-memory limits. */
+pj_status pj_plan_default(const pj_join_desc* desc, pj_plan* plan);
+
+/* Bytes of device workspace that pj_inner_join / pj_join_count need for
+ * this join and plan (plan NULL: the default plan).  The workspace must be
+ * 256-byte aligned. */
+pj_status pj_workspace_size(const pj_join_desc* desc, const pj_plan* plan, size_t* bytes);
+
+/* Exact-histogram planner: histograms both key columns on the device,
+ * reads the histograms back (SYNCHRONISES the stream) and returns a plan in
+ * which every partition's table fits shared memory.  Replaces the
+ * reference's fixed -n/-N choice and handle_skewed_data's sizing
+ * (skewed_data_handler.cuh:59-91). */
+pj_status pj_plan_exact(const pj_join_desc* desc, void* workspace, size_t workspace_bytes,
+                        pj_plan* plan, pj_stream stream);
+
+/* The join: partition both sides, build and probe per partition, write
+ * (build_row, probe_row) pairs.  Replaces main.cu:762-892.  Asynchronous;
+ * call pj_check() to learn device-side conditions. */
+pj_status pj_inner_join(const pj_join_desc* desc, const pj_plan* plan, pj_output* out,
+                        void* workspace, size_t workspace_bytes, pj_stream stream);
+
+/* Number of matching pairs only (written to *count_dev, a device int64);
+ * the count the reference takes from its CPU run (main.cu:697-704). */
+pj_status pj_join_count(const pj_join_desc* desc, const pj_plan* plan, int64_t* count_dev,
+                        void* workspace, size_t workspace_bytes, pj_stream stream);
+
+/* Stage timers of pj_inner_join, like the reference's per-stage cudaEvent
+ * timers and CSV columns (main.cu:769-896, 918-948). */
+enum {
+    PJ_STAGE_BUILD_HIST = 0,
+    PJ_STAGE_BUILD_SCAN = 1,
+    PJ_STAGE_BUILD_SCATTER = 2,
+    PJ_STAGE_PROBE_HIST = 3,
+    PJ_STAGE_PROBE_SCAN = 4,
+    PJ_STAGE_PROBE_SCATTER = 5,
+    PJ_STAGE_JOIN_PLAN = 6,  /* work split: the reference's handle_skewed_data */
+    PJ_STAGE_JOIN = 7,
+    PJ_STAGE_TOTAL = 8,
+    PJ_NUM_STAGES = 9
+};
+
+/* pj_inner_join with a cudaEvent around every stage; SYNCHRONISES the
+ * stream and writes the milliseconds of each stage to stage_ms[PJ_NUM_STAGES]. */
+pj_status pj_inner_join_timed(const pj_join_desc* desc, const pj_plan* plan, pj_output* out,
+                              void* workspace, size_t workspace_bytes, pj_stream stream,
+                              float* stage_ms);
+
+/* pj_inner_join recording events[i] (a cudaEvent_t, created by the caller)
+ * on the stream at the start of stage i and events[PJ_STAGE_TOTAL] at the
+ * end; asynchronous.  Lets a caller time every kernel inside a timed loop. */
+pj_status pj_inner_join_events(const pj_join_desc* desc, const pj_plan* plan, pj_output* out,
+                               void* workspace, size_t workspace_bytes, pj_stream stream,
+                               void* const* events);
+
+/* SYNCHRONISES the stream and returns the device-side status of the last
+ * call that used this workspace (PJ_OK, PJ_ERR_CAPACITY, PJ_ERR_OVERFLOW,
+ * PJ_ERR_TIMEOUT or PJ_ERR_INTERNAL), then clears it. */
+pj_status pj_check(void* workspace, pj_stream stream);
+
+/* ---- stage entry points (each replaces one reference stage) ------------- */
+
+/* MurmurHash3_32 (seed 0) of every key: MurmurHash3_32<K>::operator(),
+ * hash_functions.cuh:80-119.  out: n uint32 (device). */
+pj_status pj_hash_keys(const void* keys, int64_t n, int32_t key_bytes, uint32_t* out,
+                       pj_stream stream);
+
+/* Table slot of every key for a table of table_slots slots under
+ * slot_mode (PJ_SLOT_REF = hash_join_kernels.cuh:100-101).  For
+ * PJ_SLOT_FAST, skip_bits top hash bits are treated as already consumed by
+ * partition digits.  out: n int32 (device). */
+pj_status pj_hash_slots(const void* keys, int64_t n, int32_t key_bytes, int32_t table_slots,
+                        int32_t slot_mode, int32_t skip_bits, int32_t* out, pj_stream stream);
+
+/* Global digit histogram in one read of the keys: the reference's
+ * histogram_pass_one (partition_kernels.cuh:141-194) for which == 1,
+ * histogram_pass_two's global sum (:329-406) for which == 2 and
+ * combined_histogram_pass / big_histogram (:86-124, partitioned_join.cuh:22-48)
+ * for which == 0 (all bits1+bits2 digit bits).  hist: 2^bits int32 (device),
+ * overwritten. */
+pj_status pj_radix_histogram(const void* keys, int64_t n, int32_t key_bytes, int32_t digit_mode,
+                             int32_t bits1, int32_t bits2, int32_t which, int32_t* hist,
+                             pj_stream stream);
+
+/* Radix-partitions one key column into `tuples` (device, capacity
+ * pj_partitioned_capacity() tuples) with partition p occupying tuples
+ * [offsets[p], offsets[p+1]) (offsets: device int64, 2^(bits1+bits2)+1).
+ * A tuple is {int32 key, int32 row} for 4-byte keys and {int32 key_lo,
+ * int32 key_hi, int32 row} for 8-byte keys; padding tuples carry row = -1.
+ * Replaces partition_input_tables_pass_one / _pass_two
+ * (partitioned_join.cuh:51-175). */
+pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_plan* plan,
+                       void* tuples, int64_t* offsets, void* workspace, size_t workspace_bytes,
+                       pj_stream stream);
+
+/* Capacity in tuples that pj_partition needs for n keys under plan. */
+pj_status pj_partitioned_capacity(int64_t n, int32_t key_bytes, const pj_plan* plan,
+                                  int64_t* tuples);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PJ_H */

@@ -1,0 +1,78 @@
+"""C ABI checks that need no GPU: the library loads, exports every function
+include/pj.h declares, plans from sizes and rejects bad arguments."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "pj.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pj_[a-z_0-9]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    from partitioned_join_b200 import _lib
+    return _lib.lib()
+
+
+def test_header_symbols_exported(L):
+    names = header_functions()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(L, n), f"libpj.so does not export {n}"
+
+
+def test_binding_covers_header():
+    from partitioned_join_b200 import _lib
+    assert set(header_functions()) == set(_lib.SIGNATURES)
+
+
+def test_status_strings(L):
+    for s in range(9):
+        assert L.pj_status_string(s)
+    assert b"sm_100a" in L.pj_version()
+
+
+def test_plan_default_sizes():
+    from partitioned_join_b200 import api
+    p = api.plan_default(1 << 27, 1 << 27, 4)
+    assert p.passes == 1 and p.table_slots > 0
+    # every partition (at the expected size) fits the tables of its splits
+    cap = int(p.table_slots * p.max_fill)
+    assert (1 << 27) / (1 << p.bits1) <= cap * 64
+    small = api.plan_default(1000, 4000, 4)
+    assert small.bits1 == 0
+
+
+def test_workspace_size_grows_with_input():
+    from partitioned_join_b200 import api
+    a = api.workspace_size(api.desc_for_sizes(1 << 20, 1 << 22))
+    b = api.workspace_size(api.desc_for_sizes(1 << 24, 1 << 24))
+    assert 0 < a < b
+
+
+def test_invalid_arguments_rejected(L):
+    from partitioned_join_b200 import _lib, api
+    d = api.desc_for_sizes(100, 100, 4)
+    d.key_bytes = 3
+    p = _lib.Plan()
+    assert L.pj_plan_default(ctypes.byref(d), ctypes.byref(p)) == _lib.ERR_INVALID
+    d = api.desc_for_sizes(100, 100, 4)
+    n = ctypes.c_size_t()
+    bad = api.plan_default(100, 100, 4)
+    bad.passes = 3
+    assert L.pj_workspace_size(ctypes.byref(d), ctypes.byref(bad), ctypes.byref(n)) == _lib.ERR_INVALID
+    bad = api.plan_default(100, 100, 4)
+    bad.table_slots = 1 << 30
+    assert L.pj_workspace_size(ctypes.byref(d), ctypes.byref(bad), ctypes.byref(n)) == _lib.ERR_INVALID
+    # the join refuses a workspace that is missing
+    out = _lib.Output()
+    out.count = 16
+    assert L.pj_inner_join(ctypes.byref(d), None, ctypes.byref(out), None, 0, None) == _lib.ERR_WORKSPACE
+    assert L.pj_hash_keys(None, 10, 4, None, None) == _lib.ERR_INVALID

@@ -1,0 +1,228 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference's golden vectors.  Bit-exact: integer and index work."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle
+from partitioned_join_b200 import DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, PJError
+from partitioned_join_b200 import api, datagen
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def pairs_equal(b, p, br, pr, unique=True):
+    """Sorted multiset of (build_row, probe_row) equals the oracle's."""
+    eb, ep = oracle.inner_join(b, p, unique)
+    got = oracle.sorted_pairs(br.cpu().numpy(), pr.cpu().numpy())
+    exp = oracle.sorted_pairs(eb, ep)
+    return got.shape == exp.shape and np.array_equal(got, exp)
+
+
+def run(b, p, unique=True, plan=None):
+    br, pr = api.partitioned_join(dev(b), dev(p), unique_build_keys=unique, plan=plan)
+    torch.cuda.synchronize()
+    return br, pr
+
+
+# ---------------------------------------------------------------------------
+# hash, slot and digit functions against the reference's golden vectors
+
+def test_hash_matches_reference_golden(golden):
+    for kind in ("i32", "i64"):
+        keys = golden[f"hash_{kind}_keys"]
+        got = api.hash_keys(dev(keys)).cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, golden[f"hash_{kind}"]), kind
+
+
+def test_ref_slot_matches_oracle():
+    rng = np.random.default_rng(5)
+    keys = rng.integers(-(1 << 31), 1 << 31, size=20000).astype(np.int32)
+    h = oracle.hash_keys(keys)
+    for T in (1, 7, 1000, 12289, 16384, 2**31 - 1):
+        got = api.hash_slots(dev(keys), T, SLOT_REF).cpu().numpy()
+        exp = np.array([oracle.ref_slot(int(x), T) for x in h[:2000]])
+        assert np.array_equal(got[:2000], exp), T
+        assert got.min() >= 0 and got.max() < T
+
+
+def test_fast_slot_in_range():
+    rng = np.random.default_rng(6)
+    keys = rng.integers(-(1 << 62), 1 << 62, size=50000, dtype=np.int64)
+    for T, skip in ((1000, 0), (16384, 12), (8191, 20)):
+        got = api.hash_slots(dev(keys), T, SLOT_FAST, skip).cpu().numpy()
+        h = oracle.hash_keys(keys).astype(np.uint64)
+        exp = (((h << np.uint64(skip)) & np.uint64(0xFFFFFFFF)) * np.uint64(T)) >> np.uint64(32)
+        assert np.array_equal(got.astype(np.uint64), exp)
+
+
+@pytest.mark.parametrize("mode", [DIGIT_RAW, DIGIT_HASH])
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+def test_radix_histogram_matches_oracle(mode, dtype):
+    rng = np.random.default_rng(7)
+    info = np.iinfo(dtype)
+    keys = rng.integers(info.min, info.max, size=300001, dtype=dtype)
+    for b1, b2, which in ((0, 0, 0), (1, 0, 0), (10, 0, 0), (5, 3, 1), (5, 3, 2), (6, 6, 0), (14, 0, 0)):
+        got = api.radix_histogram(dev(keys), mode, b1, b2, which).cpu().numpy()
+        exp = oracle.histogram(keys, mode, b1, b2, which)
+        assert np.array_equal(got, exp), (b1, b2, which)
+
+
+# ---------------------------------------------------------------------------
+# the partition stage: every partition holds exactly the rows whose digit it is
+
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+@pytest.mark.parametrize("bits", [0, 3, 9])
+@pytest.mark.parametrize("mode", [DIGIT_RAW, DIGIT_HASH])
+def test_partition_stage_exact(dtype, bits, mode):
+    rng = np.random.default_rng(8 + bits)
+    n = 200003
+    info = np.iinfo(dtype)
+    keys = rng.integers(info.min // 2, info.max // 2, size=n, dtype=dtype)
+    plan = api.plan_default(n, n, np.dtype(dtype).itemsize)
+    plan.bits1 = bits
+    plan.digit_mode = mode
+    tuples, offsets = api.partition(dev(keys), plan)
+    t = tuples.cpu().numpy()
+    off = offsets.cpu().numpy()
+    words = 2 if dtype == np.int32 else 3
+    P = 1 << bits
+    assert off[0] == 0 and np.all(np.diff(off) >= 0)
+    rec = t[: off[-1] * words].reshape(-1, words)
+    rows = rec[:, -1]
+    if dtype == np.int32:
+        k = rec[:, 0].astype(np.int32)
+    else:
+        k = (rec[:, 1].astype(np.int64) << 32) | (rec[:, 0].astype(np.int64) & 0xFFFFFFFF)
+    real = rows >= 0
+    assert np.all(rows[~real] == -1)
+    # every input row exactly once, carrying its own key
+    assert np.array_equal(np.sort(rows[real]), np.arange(n))
+    assert np.array_equal(k[real], keys[rows[real]])
+    # every row sits in its digit's partition
+    part = np.repeat(np.arange(P), np.diff(off))
+    d = oracle.digits(keys, mode, bits, 0, 0)
+    assert np.array_equal(part[real], d[rows[real]])
+
+
+# ---------------------------------------------------------------------------
+# full join parity against the oracle
+
+@pytest.mark.parametrize("case", ["i32_unique", "i32_multi", "i32_unique_flag_dups", "i32_edges",
+                                  "i64_unique_zipf", "i64_multi", "i32_nomatch", "i32_single"])
+def test_join_golden_cases(golden, case):
+    b = golden[f"join_{case}_build"]
+    p = golden[f"join_{case}_probe"]
+    uniq = bool(golden[f"join_{case}_unique"])
+    br, pr = run(b, p, uniq)
+    bk = b[br.cpu().numpy()]
+    # key projection equals the reference inner_join_cpu's record multiset
+    assert np.array_equal(np.sort(bk), golden[f"join_{case}_keys"])
+    if case != "i32_unique_flag_dups":
+        assert pairs_equal(b, p, br, pr, uniq)
+    else:
+        # repeated keys under the unique flag: each probe row matches one of them
+        assert np.array_equal(b[br.cpu().numpy()], p[pr.cpu().numpy()])
+
+
+def test_join_config1_shape_scaled():
+    b, p = datagen.config1(seed=11, n_build=1 << 18, n_probe=1 << 20)
+    br, pr = run(b, p)
+    assert br.numel() == p.shape[0]
+    assert pairs_equal(b, p, br, pr)
+
+
+def test_join_config2_shape_scaled():
+    b, p = datagen.config2(seed=12, n_build=1 << 21, n_probe=1 << 21)
+    br, pr = run(b, p)
+    assert pairs_equal(b, p, br, pr)
+
+
+@pytest.mark.parametrize("digit", [DIGIT_RAW, DIGIT_HASH])
+@pytest.mark.parametrize("slot", [SLOT_FAST, SLOT_REF])
+@pytest.mark.parametrize("split", [SPLIT_HASH, SPLIT_POSITION])
+def test_join_plan_variants(digit, slot, split):
+    b, p = datagen.config2(seed=13, n_build=300000, n_probe=500000)
+    plan = api.plan_default(b.shape[0], p.shape[0], 4)
+    plan.digit_mode, plan.slot_mode, plan.split_mode = digit, slot, split
+    plan.bits1 = 3                  # coarse: forces 2..8 pieces per partition
+    plan.table_slots = 8192
+    plan.probe_chunk = 4096         # several probe chunks per partition
+    br, pr = run(b, p, True, plan)
+    assert pairs_equal(b, p, br, pr)
+
+
+def test_join_int64_skewed():
+    b, p = datagen.config3(seed=14, theta=1.25, n_build=1 << 17, n_probe=1 << 19)
+    br, pr = run(b, p)
+    assert pairs_equal(b, p, br, pr)
+
+
+def test_join_multimap_heavy_duplicates():
+    rng = np.random.default_rng(15)
+    b = np.concatenate([np.full(5000, 77, np.int32), rng.integers(0, 20000, size=30000).astype(np.int32)])
+    p = np.concatenate([np.full(300, 77, np.int32), rng.integers(0, 30000, size=60000).astype(np.int32)])
+    br, pr = run(b, p, unique=False)
+    assert pairs_equal(b, p, br, pr, unique=False)
+
+
+def test_join_all_probes_one_key():
+    b = np.arange(1, 100001, dtype=np.int32)
+    p = np.full(400000, 4242, dtype=np.int32)
+    br, pr = run(b, p)
+    assert pairs_equal(b, p, br, pr)
+
+
+def test_join_sentinel_keys_join():
+    # -1 is the reference's empty-slot marker; here it is an ordinary key
+    b = np.array([-1, 0, 1, -2**31, 2**31 - 1], dtype=np.int32)
+    p = np.array([-1, -1, 2**31 - 1, 5, 0, -2**31], dtype=np.int32)
+    br, pr = run(b, p)
+    assert pairs_equal(b, p, br, pr)
+
+
+def test_join_empty_sides():
+    e = np.zeros(0, np.int32)
+    x = np.arange(100, dtype=np.int32)
+    for b, p in ((e, x), (x, e), (e, e)):
+        br, pr = run(b, p)
+        assert br.numel() == 0 and pr.numel() == 0
+
+
+def test_join_ragged_sizes():
+    rng = np.random.default_rng(16)
+    for nb, np_ in ((1, 1), (3, 17), (15, 33), (1023, 4097), (70001, 130003)):
+        b = rng.permutation(nb * 3)[:nb].astype(np.int32)
+        p = rng.integers(0, nb * 3, size=np_).astype(np.int32)
+        br, pr = run(b, p)
+        assert pairs_equal(b, p, br, pr), (nb, np_)
+
+
+def test_capacity_error_reports_required_count():
+    b = np.arange(1000, dtype=np.int32)
+    p = np.tile(np.arange(1000, dtype=np.int32), 3)
+    j = api.Joiner(dev(b), dev(p), True, capacity=10)
+    j.launch()
+    with pytest.raises(PJError) as e:
+        j.result()
+    assert int(j.count.item()) == 3000
+    assert "capacity" in str(e.value)
+
+
+def test_join_count_matches_oracle():
+    b, p = datagen.config2(seed=17, n_build=100000, n_probe=200000)
+    assert api.join_count(dev(b), dev(p)) == oracle.inner_join(b, p)[0].shape[0]
+
+
+def test_misaligned_input_rejected():
+    b = dev(np.arange(101, dtype=np.int32))
+    p = dev(np.arange(100, dtype=np.int32))
+    with pytest.raises(PJError) as e:
+        api.partitioned_join(b[1:], p)
+    assert e.value.status == 7
