@@ -34,6 +34,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "tuples/s & HBM-roofline %, 2^27x2^27 int32 join"
+# kernels of one pj_inner_join: per side histogram, scan, scatter; then
+# join_items, scan, items_expand, join
+LAUNCHES_PER_JOIN = 10
 UNIT = "tuples/s"
 
 
@@ -52,6 +55,7 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plan", type=str, default="", help="JSON overrides of pj_plan fields")
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--default-plan", action="store_true", help="plan from sizes only (no histogram)")
     return ap.parse_args()
 
 
@@ -223,7 +227,8 @@ def run_ours(args, rank, world, local):
 
     n_b, n_p = 1 << args.log2_build, 1 << args.log2_probe
     build, probe, expected = gen_config2_device(n_b, n_p, args.match_rate, args.seed + rank, device)
-    plan = api.plan_default(n_b, n_p, 4, True)
+    # the exact-histogram planner picks the digit source (and split) from the data
+    plan = api.plan_exact(build, probe, True) if not args.default_plan else api.plan_default(n_b, n_p, 4, True)
     if args.plan:
         for k, v in json.loads(args.plan).items():
             setattr(plan, k, v)
@@ -303,7 +308,7 @@ def run_ours(args, rank, world, local):
                    "l2": "inputs (1 GiB) larger than L2, no flush", "parallelism": f"replicas x{world}",
                    "plan": plan.as_dict()},
         "clocks": clk,
-        "gpu_launches": 9 * args.steps,
+        "gpu_launches": LAUNCHES_PER_JOIN * args.steps,
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": f"{kernel_of[dom]} ({dom})", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,

@@ -98,24 +98,31 @@ typedef struct pj_output {
     void* probe_payload_out;    /* optional: probe_payload[probe_row[i]] */
 } pj_output;
 
+/* Shared-memory table of the join. */
+enum {
+    PJ_TABLE_BUCKET = 0,  /* build tuples counting-sorted by hash bucket (8 B a tuple) */
+    PJ_TABLE_OPEN = 1     /* the reference's open addressing, linear probing,
+                             hash_join_kernels.cuh:19-129 */
+};
+
 /* Execution plan.  pj_plan_default() fills it from the sizes alone,
- * pj_plan_exact() from an exact device histogram.  Passing NULL to
- * pj_inner_join() uses pj_plan_default(). */
+ * pj_plan_exact() from device histograms.  Passing NULL to pj_inner_join()
+ * uses pj_plan_default(). */
 typedef struct pj_plan {
-    int32_t passes;             /* 1 or 2 radix passes */
-    int32_t bits1;              /* radix bits of pass 1 */
-    int32_t bits2;              /* radix bits of pass 2 (0 when passes == 1) */
+    int32_t passes;             /* radix passes (1) */
+    int32_t bits1;              /* radix bits of pass 1: 2^bits1 partitions */
+    int32_t bits2;              /* radix bits of pass 2 (0) */
     int32_t digit_mode;         /* PJ_DIGIT_* */
-    int32_t slot_mode;          /* PJ_SLOT_* */
+    int32_t table_mode;         /* PJ_TABLE_* */
+    int32_t slot_mode;          /* PJ_SLOT_* (PJ_TABLE_OPEN) */
     int32_t split_mode;         /* PJ_SPLIT_* */
-    int32_t table_slots;        /* slots of one shared-memory table */
-    int32_t probe_chunk;        /* probe rows of one join work item */
-    int32_t join_threads;       /* threads per join CTA */
-    int32_t scatter_threads;    /* threads per scatter CTA */
-    int32_t scatter_ctas_per_sm;/* resident scatter CTAs per SM (its chunks) */
+    int32_t table_capacity;     /* BUCKET: build tuples one table holds; OPEN: slots */
+    int32_t probe_chunk;        /* probe tuples of one join work item (multiple of 16) */
+    int32_t wc_tuples;          /* tuples per write-combining buffer: 2, 4 or 8 */
+    int32_t scatter_ctas_per_sm;/* scatter chunks per SM */
+    int32_t hist_split;         /* histogram CTAs per scatter chunk */
+    float max_fill;             /* OPEN: target fill (the reference's HASH_TABLE_OCC = 0.5) */
     int32_t flags;              /* reserved, 0 */
-    float max_fill;             /* target table fill (the reference's HASH_TABLE_OCC = 0.5) */
-    float reserved_f;
 } pj_plan;
 
 /* Human-readable text of a status. */

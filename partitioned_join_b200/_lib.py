@@ -13,6 +13,7 @@ OK, ERR_INVALID, ERR_CAPACITY, ERR_CUDA, ERR_TIMEOUT, ERR_WORKSPACE, ERR_OVERFLO
 DIGIT_RAW, DIGIT_HASH = 0, 1
 SLOT_FAST, SLOT_REF = 0, 1
 SPLIT_HASH, SPLIT_POSITION = 0, 1
+TABLE_BUCKET, TABLE_OPEN = 0, 1
 STAGES = ["build_hist", "build_scan", "build_scatter", "probe_hist", "probe_scan", "probe_scatter", "join_plan",
           "join", "total"]
 
@@ -33,10 +34,10 @@ class Output(ctypes.Structure):
 
 class Plan(ctypes.Structure):
     _fields_ = [("passes", ctypes.c_int32), ("bits1", ctypes.c_int32), ("bits2", ctypes.c_int32),
-                ("digit_mode", ctypes.c_int32), ("slot_mode", ctypes.c_int32), ("split_mode", ctypes.c_int32),
-                ("table_slots", ctypes.c_int32), ("probe_chunk", ctypes.c_int32), ("join_threads", ctypes.c_int32),
-                ("scatter_threads", ctypes.c_int32), ("scatter_ctas_per_sm", ctypes.c_int32),
-                ("flags", ctypes.c_int32), ("max_fill", ctypes.c_float), ("reserved_f", ctypes.c_float)]
+                ("digit_mode", ctypes.c_int32), ("table_mode", ctypes.c_int32), ("slot_mode", ctypes.c_int32),
+                ("split_mode", ctypes.c_int32), ("table_capacity", ctypes.c_int32), ("probe_chunk", ctypes.c_int32),
+                ("wc_tuples", ctypes.c_int32), ("scatter_ctas_per_sm", ctypes.c_int32), ("hist_split", ctypes.c_int32),
+                ("max_fill", ctypes.c_float), ("flags", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

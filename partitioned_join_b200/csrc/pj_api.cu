@@ -20,14 +20,15 @@ namespace {
 // ---------------------------------------------------------------------------
 // Fixed kernel configurations.
 constexpr int SC_THREADS = 1024;
-constexpr int SC_NSTAGE = 3;
-constexpr int SC_V32 = 4, SC_V64 = 2;   // keys per thread per round: 16 KB stages
-constexpr int SC_W32 = 4, SC_W64 = 8;   // tuples per write-combining buffer: 32 B / 96 B
+constexpr int SC_V32 = 4, SC_V64 = 2;  // keys per thread per round (one 16-byte vector)
+#ifndef PJ_JOIN_THREADS
 constexpr int JN_THREADS = 1024;
-constexpr int JN_OB = 4096;
-constexpr int JN_NSTAGE = 3;
-constexpr int JN_STAGE_TUPLES = 2048;
+#else
+constexpr int JN_THREADS = PJ_JOIN_THREADS;
+#endif
 constexpr int MAX_SPLIT_LOG2 = 6;
+constexpr int MAX_BUCKET_CAP = 65535;  // 16-bit bucket ends
+constexpr int MAX_JOIN_CTAS_PER_SM = 4;
 
 struct DevInfo {
     int device = -1;
@@ -40,16 +41,19 @@ DevInfo dev_info()
     static std::mutex mu;
     static DevInfo cache[64];
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return DevInfo{};
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return DevInfo{};
+    }
     std::lock_guard<std::mutex> lock(mu);
     if (dev >= 0 && dev < 64 && cache[dev].device == dev) return cache[dev];
     DevInfo d;
     d.device = dev;
     int v = 0;
-    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-    d.sms = v;
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    d.smem_optin = static_cast<size_t>(v);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) d.sms = v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
+        d.smem_optin = static_cast<size_t>(v);
+    cudaGetLastError();
     if (dev >= 0 && dev < 64) cache[dev] = d;
     return d;
 }
@@ -62,10 +66,18 @@ int sm_count()
     return d.sms > 0 ? d.sms : 148;
 }
 
+// Dynamic shared memory per CTA, less a reserve for static shared memory.
 size_t smem_limit()
 {
     const DevInfo d = dev_info();
-    return d.smem_optin > 0 ? d.smem_optin : 232448;
+    return (d.smem_optin > 0 ? d.smem_optin : 232448) - 1024;
+}
+
+int ilog2_floor(int64_t x)
+{
+    int b = 0;
+    while ((int64_t(2) << b) <= x) ++b;
+    return b;
 }
 
 int ilog2_ceil(int64_t x)
@@ -79,40 +91,47 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 template <typename K>
 constexpr int sc_v() { return sizeof(K) == 4 ? SC_V32 : SC_V64; }
-template <typename K>
-constexpr int sc_w() { return sizeof(K) == 4 ? SC_W32 : SC_W64; }
 
-template <typename K>
-size_t scatter_smem(int P)
+int tuple_words(int key_bytes) { return key_bytes == 4 ? 2 : 3; }
+
+size_t scatter_smem(int key_bytes, int W, int P)
 {
-    return ScatterSmem<K, SC_THREADS, sc_v<K>(), sc_w<K>(), SC_NSTAGE>::bytes(P);
+    return static_cast<size_t>(P) * W * tuple_words(key_bytes) * 4 + static_cast<size_t>(P) * 8;
 }
 
-template <typename K>
-size_t join_smem(int T)
+bool valid_wc(int key_bytes, int W)
 {
-    return JoinSmem<K, JN_THREADS, JN_OB, JN_NSTAGE, JN_STAGE_TUPLES>::bytes(T);
+    if (W != 2 && W != 4 && W != 8) return false;
+    return (W * tuple_words(key_bytes) * 4) % 16 == 0;
 }
 
-int max_one_pass_bits(int key_bytes)
+// Groups that are whole 32-byte sectors: the planner's choice.  Smaller
+// groups are valid but leave sectors half written in L2 until a later
+// flush, which measured at twice the DRAM traffic.
+bool sector_wc(int key_bytes, int W) { return valid_wc(key_bytes, W) && (W * tuple_words(key_bytes) * 4) % 32 == 0; }
+
+int bucket_nb_log2(int cap) { return std::max(1, ilog2_floor(std::max(2, cap / 2))); }
+
+size_t join_smem(int key_bytes, int table_mode, int cap)
 {
-    int b = 0;
+    const int nb = bucket_nb_log2(cap);
+    if (key_bytes == 4)
+        return table_mode == PJ_TABLE_BUCKET ? JoinSmem<int32_t, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS)
+                                             : JoinSmem<int32_t, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
+    return table_mode == PJ_TABLE_BUCKET ? JoinSmem<int64_t, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS)
+                                         : JoinSmem<int64_t, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
+}
+
+int max_table_capacity(int key_bytes, int table_mode)
+{
+    int lo = 64, hi = table_mode == PJ_TABLE_BUCKET ? MAX_BUCKET_CAP : (1 << 20);
     const size_t lim = smem_limit();
-    for (int t = 1; t <= 16; ++t) {
-        const size_t s = key_bytes == 4 ? scatter_smem<int32_t>(1 << t) : scatter_smem<int64_t>(1 << t);
-        if (s <= lim) b = t;
+    if (join_smem(key_bytes, table_mode, lo) > lim) return 0;
+    while (lo < hi) {  // largest cap that fits
+        const int mid = lo + (hi - lo + 1) / 2;
+        if (join_smem(key_bytes, table_mode, mid) <= lim) lo = mid; else hi = mid - 1;
     }
-    return b;
-}
-
-int max_table_slots(int key_bytes)
-{
-    const size_t lim = smem_limit();
-    const size_t base = key_bytes == 4 ? join_smem<int32_t>(0) : join_smem<int64_t>(0);
-    const int slot = key_bytes == 4 ? 8 : 12;
-    if (lim <= base + 1024) return 0;
-    int T = static_cast<int>((lim - base - 512) / slot);
-    return T & ~127;
+    return lo & ~127;
 }
 
 bool valid_desc(const pj_join_desc* d)
@@ -130,17 +149,32 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
 {
-    if (p->passes != 1) return PJ_ERR_INVALID;
-    if (p->bits1 < 0 || p->bits1 > max_one_pass_bits(d->key_bytes)) return PJ_ERR_INVALID;
+    if (p->passes != 1 || p->bits2 != 0) return PJ_ERR_INVALID;
+    if (p->bits1 < 0 || p->bits1 > 16) return PJ_ERR_INVALID;
+    if (!valid_wc(d->key_bytes, p->wc_tuples)) return PJ_ERR_INVALID;
+    if (scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) > smem_limit()) return PJ_ERR_INVALID;
     if (p->digit_mode != PJ_DIGIT_RAW && p->digit_mode != PJ_DIGIT_HASH) return PJ_ERR_INVALID;
+    if (p->table_mode != PJ_TABLE_BUCKET && p->table_mode != PJ_TABLE_OPEN) return PJ_ERR_INVALID;
     if (p->slot_mode != PJ_SLOT_FAST && p->slot_mode != PJ_SLOT_REF) return PJ_ERR_INVALID;
     if (p->split_mode != PJ_SPLIT_HASH && p->split_mode != PJ_SPLIT_POSITION) return PJ_ERR_INVALID;
-    if (p->table_slots < 64 || p->table_slots > max_table_slots(d->key_bytes)) return PJ_ERR_INVALID;
+    if (p->table_capacity < 64 || p->table_capacity > max_table_capacity(d->key_bytes, p->table_mode))
+        return PJ_ERR_INVALID;
     if (p->probe_chunk < 16 || (p->probe_chunk & 15)) return PJ_ERR_INVALID;
-    if (!(p->max_fill > 0.05f && p->max_fill <= 0.95f)) return PJ_ERR_INVALID;
-    const int used = (p->digit_mode == PJ_DIGIT_HASH ? p->bits1 + p->bits2 : 0) + MAX_SPLIT_LOG2;
-    if (used > 26) return PJ_ERR_INVALID;
+    if (p->scatter_ctas_per_sm < 1 || p->scatter_ctas_per_sm > 8) return PJ_ERR_INVALID;
+    if (p->hist_split < 1 || p->hist_split > 16) return PJ_ERR_INVALID;
+    if (p->table_mode == PJ_TABLE_OPEN && !(p->max_fill > 0.05f && p->max_fill <= 0.95f)) return PJ_ERR_INVALID;
+    // hash bits: digits + hash split + bucket/slot bits must fit 32
+    const int digit_bits = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0;
+    const int slot_bits = p->table_mode == PJ_TABLE_BUCKET ? bucket_nb_log2(p->table_capacity) : 12;
+    if (digit_bits + MAX_SPLIT_LOG2 + slot_bits > 32) return PJ_ERR_INVALID;
     return PJ_OK;
+}
+
+// Build tuples one table holds.
+int table_tuples(const pj_plan* p)
+{
+    return p->table_mode == PJ_TABLE_BUCKET ? p->table_capacity
+                                            : std::max(1, static_cast<int>(p->table_capacity * p->max_fill));
 }
 
 // ---------------------------------------------------------------------------
@@ -150,8 +184,13 @@ struct Layout {
     int b_items = 1, p_items = 1;
     int64_t b_chunk = 16, p_chunk = 16;
     int64_t b_cap = 0, p_cap = 0;  // tuples
-    size_t status = 0, counters = 0, b_tiles = 0, p_tiles = 0, i_tiles = 0, b_tot = 0, p_tot = 0, ctrl_end = 0;
-    size_t b_counts = 0, p_counts = 0, b_off = 0, p_off = 0, split = 0, items = 0, item_off = 0;
+    int64_t max_items = 0;
+    size_t status = 0, counters = 0, b_tiles = 0, p_tiles = 0, i_tiles = 0, b_tot = 0, p_tot = 0;
+    size_t b_counts = 0, p_counts = 0, ctrl_end = 0;
+    size_t b_off = 0, p_off = 0, split = 0, items = 0, item_off = 0, item_part = 0;
+    size_t cta_q = 0, cta_last = 0, seg = 0, over_b = 0, over_p = 0;
+    int max_ctas = 0;
+    int64_t over_cap = 0;
     size_t b_tuples = 0, p_tuples = 0, total = 0;
     int64_t b_tiles_n = 0, p_tiles_n = 0, i_tiles_n = 0;
 };
@@ -167,11 +206,7 @@ int64_t chunk_for(int64_t n, int items)
 
 int scatter_items(const pj_plan* p) { return sm_count() * std::max(1, p->scatter_ctas_per_sm); }
 
-int64_t part_capacity(int64_t n, int key_bytes, int P, int items)
-{
-    const int W = key_bytes == 4 ? SC_W32 : SC_W64;
-    return n + static_cast<int64_t>(items) * P * (W - 1) + W;
-}
+int64_t part_capacity(int64_t n, int P, int items, int W) { return n + static_cast<int64_t>(items) * P * (W - 1) + W; }
 
 Layout make_layout(const pj_join_desc* d, const pj_plan* p)
 {
@@ -180,15 +215,22 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.b_items = L.p_items = scatter_items(p);
     L.b_chunk = chunk_for(d->n_build, L.b_items);
     L.p_chunk = chunk_for(d->n_probe, L.p_items);
-    L.b_cap = part_capacity(d->n_build, d->key_bytes, L.P, L.b_items);
-    L.p_cap = part_capacity(d->n_probe, d->key_bytes, L.P, L.p_items);
+    L.b_cap = part_capacity(d->n_build, L.P, L.b_items, p->wc_tuples);
+    L.p_cap = part_capacity(d->n_probe, L.P, L.p_items, p->wc_tuples);
     const int64_t mb = static_cast<int64_t>(L.P) * L.b_items, mp = static_cast<int64_t>(L.P) * L.p_items;
     L.b_tiles_n = (mb + SCAN_TILE - 1) / SCAN_TILE + 1;
     L.p_tiles_n = (mp + SCAN_TILE - 1) / SCAN_TILE + 1;
     L.i_tiles_n = (L.P + SCAN_TILE - 1) / SCAN_TILE + 1;
+    // items: per partition at most 2^MAX_SPLIT_LOG2 hash pieces, or
+    // table-sized position pieces, times ceil(probe range / probe_chunk)
+    const int64_t per_piece = std::max<int64_t>(16, table_tuples(p) / 16 * 16);
+    const int64_t max_pieces = std::max<int64_t>(static_cast<int64_t>(L.P) << MAX_SPLIT_LOG2, L.P + L.b_cap / per_piece);
+    const int64_t max_chunks = L.P + L.p_cap / p->probe_chunk + 1;
+    L.max_items = std::min<int64_t>(max_pieces * max_chunks, static_cast<int64_t>(L.P) * 4096 + max_pieces + max_chunks);
+    L.max_items = std::min<int64_t>(L.max_items, int64_t(1) << 30);
     size_t o = 0;
     auto take = [&](size_t bytes) { const size_t at = o; o = align_up(o + bytes, 256); return at; };
-    // control block: zeroed at the start of every call
+    // control block, zeroed at the start of every call
     L.status = take(4);
     L.counters = take(4 * 8);
     L.b_tiles = take(8 * L.b_tiles_n);
@@ -196,15 +238,25 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.i_tiles = take(8 * L.i_tiles_n);
     L.b_tot = take(4 * static_cast<size_t>(L.P));
     L.p_tot = take(4 * static_cast<size_t>(L.P));
-    L.ctrl_end = o;
     L.b_counts = take(4 * static_cast<size_t>(mb));
     L.p_counts = take(4 * static_cast<size_t>(mp));
+    L.ctrl_end = o;
     L.b_off = take(8 * static_cast<size_t>(mb + 1));
     L.p_off = take(8 * static_cast<size_t>(mp + 1));
     L.split = take(4 * static_cast<size_t>(L.P));
     L.items = take(8 * static_cast<size_t>(L.P));
     L.item_off = take(8 * static_cast<size_t>(L.P + 1));
-    const int TW = d->key_bytes == 4 ? 2 : 3;
+    L.item_part = take(4 * static_cast<size_t>(L.max_items));
+    // output fix-up: per join CTA records, segments, and room for the
+    // reserved positions past the caller's capacity (one chunk per CTA)
+    L.max_ctas = sm_count() * MAX_JOIN_CTAS_PER_SM;
+    L.over_cap = static_cast<int64_t>(L.max_ctas) * OUT_CHUNK;
+    L.cta_q = take(8 * static_cast<size_t>(L.max_ctas));
+    L.cta_last = take(8 * static_cast<size_t>(L.max_ctas));
+    L.seg = take(8 * (4 + 4 * static_cast<size_t>(L.max_ctas + 2)));
+    L.over_b = take(4 * static_cast<size_t>(L.over_cap));
+    L.over_p = take(4 * static_cast<size_t>(L.over_cap));
+    const int TW = tuple_words(d->key_bytes);
     L.b_tuples = take(4 * static_cast<size_t>(TW) * L.b_cap + 64);
     L.p_tuples = take(4 * static_cast<size_t>(TW) * L.p_cap + 64);
     L.total = o;
@@ -220,6 +272,12 @@ DigitFn digit_fn(int mode, int bits_before, int bits, int raw_shift)
     return f;
 }
 
+cudaError_t& last_cuda_error()
+{
+    static thread_local cudaError_t e = cudaSuccess;
+    return e;
+}
+
 #define PJ_CUDA(call)                                            \
     do {                                                         \
         cudaError_t e_ = (call);                                 \
@@ -228,12 +286,6 @@ DigitFn digit_fn(int mode, int bits_before, int bits, int raw_shift)
             return PJ_ERR_CUDA;                                  \
         }                                                        \
     } while (0)
-
-cudaError_t& last_cuda_error()
-{
-    static thread_local cudaError_t e = cudaSuccess;
-    return e;
-}
 
 template <typename F>
 cudaError_t set_smem(F* fn, size_t bytes)
@@ -281,12 +333,19 @@ unsigned grid_for(int64_t n, int threads)
 // Stage launchers.
 
 template <typename K>
-pj_status launch_hist(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P, uint32_t* counts,
-                      int32_t* totals, uint32_t* status, cudaStream_t st)
+pj_status launch_hist(const K* keys, int64_t n, int64_t chunk, int items, int hsplit, DigitFn f, int P,
+                      uint32_t* counts, int32_t* totals, cudaStream_t st)
 {
-    const size_t smem = static_cast<size_t>(HIST_NSTAGE) * HIST_THREADS * HIST_V * sizeof(K) + 4 * static_cast<size_t>(P);
-    PJ_CUDA(set_smem(hist_keys_kernel<K>, smem));
-    hist_keys_kernel<K><<<items, HIST_THREADS, smem, st>>>(keys, n, chunk, items, f, P, counts, totals, status);
+    const size_t smem = 4 * static_cast<size_t>(P);
+    if (f.mode == PJ_DIGIT_HASH) {
+        PJ_CUDA(set_smem(hist_keys_kernel<K, true>, smem));
+        hist_keys_kernel<K, true><<<items * hsplit, HIST_THREADS, smem, st>>>(keys, n, chunk, items, hsplit, f, P,
+                                                                             counts, totals);
+    } else {
+        PJ_CUDA(set_smem(hist_keys_kernel<K, false>, smem));
+        hist_keys_kernel<K, false><<<items * hsplit, HIST_THREADS, smem, st>>>(keys, n, chunk, items, hsplit, f, P,
+                                                                              counts, totals);
+    }
     PJ_CUDA(cudaGetLastError());
     return PJ_OK;
 }
@@ -302,13 +361,12 @@ pj_status launch_scan(const TIn* in, int64_t m, uint32_t round_to, int64_t* out,
     return PJ_OK;
 }
 
-template <typename K>
-pj_status launch_scatter(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P,
-                         const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status, cudaStream_t st)
+template <typename K, int W, bool HASHD>
+pj_status launch_scatter_w(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P,
+                           const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status, cudaStream_t st)
 {
-    constexpr int V = sc_v<K>(), W = sc_w<K>();
-    auto* kern = scatter_keys_kernel<K, SC_THREADS, V, W, SC_NSTAGE>;
-    const size_t smem = scatter_smem<K>(P);
+    auto* kern = scatter_keys_kernel<K, SC_THREADS, sc_v<K>(), W, HASHD>;
+    const size_t smem = scatter_smem(sizeof(K), W, P);
     PJ_CUDA(set_smem(kern, smem));
     kern<<<items, SC_THREADS, smem, st>>>(keys, n, chunk, items, f, P, offsets, out,
                                          static_cast<uint32_t>(std::min<int64_t>(out_cap, UINT32_MAX)), status);
@@ -316,45 +374,71 @@ pj_status launch_scatter(const K* keys, int64_t n, int64_t chunk, int items, Dig
     return PJ_OK;
 }
 
-template <typename K, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF>
+template <typename K>
+pj_status launch_scatter(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P, int W,
+                         const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status, cudaStream_t st)
+{
+    const bool h = f.mode == PJ_DIGIT_HASH;
+    if constexpr (sizeof(K) == 4) {
+        if (W == 2)
+            return h ? launch_scatter_w<K, 2, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st)
+                     : launch_scatter_w<K, 2, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st);
+    }
+    if (W == 4)
+        return h ? launch_scatter_w<K, 4, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st)
+                 : launch_scatter_w<K, 4, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st);
+    if (W == 8)
+        return h ? launch_scatter_w<K, 8, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st)
+                 : launch_scatter_w<K, 8, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st);
+    return PJ_ERR_INVALID;
+}
+
+template <typename K, int TABLE, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF>
 pj_status launch_join_t(const JoinArgs& a, cudaStream_t st)
 {
-    auto* kern = join_kernel<K, UNIQUE, HASH_SPLIT, SLOT_REF, JN_THREADS, JN_OB, JN_NSTAGE, JN_STAGE_TUPLES>;
-    const size_t smem = join_smem<K>(a.table_slots);
+    auto* kern = join_kernel<K, TABLE, UNIQUE, HASH_SPLIT, SLOT_REF, JN_THREADS>;
+    const size_t smem = JoinSmem<K, TABLE>::bytes(a.cap, a.nb_log2, JN_THREADS);
     PJ_CUDA(set_smem(kern, smem));
     int per_sm = 0;
     PJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, JN_THREADS, smem));
-    per_sm = std::max(per_sm, 1);
-    kern<<<sm_count() * per_sm, JN_THREADS, smem, st>>>(a);
+    per_sm = std::min(std::max(per_sm, 1), MAX_JOIN_CTAS_PER_SM);
+    const int grid = sm_count() * per_sm;
+    kern<<<grid, JN_THREADS, smem, st>>>(a);
     PJ_CUDA(cudaGetLastError());
+    // fix-up: dense output and the true count
+    join_fixup_plan_kernel<<<1, 1024, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.capacity,
+                                               a.out_build != nullptr ? 1 : 0, a.seg, a.status);
+    PJ_CUDA(cudaGetLastError());
+    if (a.out_build != nullptr) {
+        join_fixup_move_kernel<<<sm_count() * 2, 512, 0, st>>>(a.seg, grid, a.out_build, a.out_probe, a.capacity,
+                                                               a.over_build, a.over_probe);
+        PJ_CUDA(cudaGetLastError());
+    }
     return PJ_OK;
 }
 
-template <typename K>
-pj_status launch_join(const JoinArgs& a, bool unique, bool hash_split, bool slot_ref, cudaStream_t st)
+template <typename K, int TABLE>
+pj_status launch_join_tab(const JoinArgs& a, bool unique, bool hash_split, bool slot_ref, cudaStream_t st)
 {
     if (unique) {
         if (hash_split)
-            return slot_ref ? launch_join_t<K, true, true, true>(a, st) : launch_join_t<K, true, true, false>(a, st);
-        return slot_ref ? launch_join_t<K, true, false, true>(a, st) : launch_join_t<K, true, false, false>(a, st);
+            return slot_ref ? launch_join_t<K, TABLE, true, true, true>(a, st)
+                            : launch_join_t<K, TABLE, true, true, false>(a, st);
+        return slot_ref ? launch_join_t<K, TABLE, true, false, true>(a, st)
+                        : launch_join_t<K, TABLE, true, false, false>(a, st);
     }
     if (hash_split)
-        return slot_ref ? launch_join_t<K, false, true, true>(a, st) : launch_join_t<K, false, true, false>(a, st);
-    return slot_ref ? launch_join_t<K, false, false, true>(a, st) : launch_join_t<K, false, false, false>(a, st);
+        return slot_ref ? launch_join_t<K, TABLE, false, true, true>(a, st)
+                        : launch_join_t<K, TABLE, false, true, false>(a, st);
+    return slot_ref ? launch_join_t<K, TABLE, false, false, true>(a, st)
+                    : launch_join_t<K, TABLE, false, false, false>(a, st);
 }
 
-// Partition one side: histogram -> scan -> scatter.
 template <typename K>
-pj_status partition_side(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P, uint32_t* counts,
-                         int32_t* totals, int64_t* off, uint64_t* tiles, uint32_t* tile_ctr, uint32_t* out,
-                         int64_t out_cap, uint32_t* status, cudaStream_t st)
+pj_status launch_join(const JoinArgs& a, int table_mode, bool unique, bool hash_split, bool slot_ref, cudaStream_t st)
 {
-    pj_status s;
-    if ((s = launch_hist<K>(keys, n, chunk, items, f, P, counts, totals, status, st)) != PJ_OK) return s;
-    if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(P) * items, static_cast<uint32_t>(sc_w<K>()), off,
-                                   tiles, tile_ctr, status, st)) != PJ_OK)
-        return s;
-    return launch_scatter<K>(keys, n, chunk, items, f, P, off, out, out_cap, status, st);
+    if (table_mode == PJ_TABLE_BUCKET) return launch_join_tab<K, TABLE_BUCKET>(a, unique, hash_split, false, st);
+    return launch_join_tab<K, TABLE_OPEN>(a, unique, hash_split, slot_ref, st);
 }
 
 // Optional stage events: ev[i] is recorded before stage i, ev[PJ_STAGE_TOTAL] at the end.
@@ -365,6 +449,31 @@ struct StageEvents {
         if (ev) cudaEventRecord(ev[i], st);
     }
 };
+
+// Partition one column: histogram -> look-back scan -> scatter.
+template <typename K>
+pj_status partition_column(const K* keys, int64_t n, const pj_plan* p, const Layout& L, int side, uint8_t* ws,
+                           uint32_t* tuples, int64_t cap, const StageEvents& E, int stage0, cudaStream_t st)
+{
+    const DigitFn f = digit_fn(p->digit_mode, 0, p->bits1, 0);
+    const int64_t chunk = side == 0 ? L.b_chunk : L.p_chunk;
+    const int items = side == 0 ? L.b_items : L.p_items;
+    uint32_t* status = reinterpret_cast<uint32_t*>(ws + L.status);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(ws + L.counters);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(ws + (side == 0 ? L.b_counts : L.p_counts));
+    int32_t* tot = reinterpret_cast<int32_t*>(ws + (side == 0 ? L.b_tot : L.p_tot));
+    int64_t* off = reinterpret_cast<int64_t*>(ws + (side == 0 ? L.b_off : L.p_off));
+    uint64_t* tiles = reinterpret_cast<uint64_t*>(ws + (side == 0 ? L.b_tiles : L.p_tiles));
+    pj_status s;
+    E.mark(stage0, st);
+    if ((s = launch_hist<K>(keys, n, chunk, items, p->hist_split, f, L.P, counts, tot, st)) != PJ_OK) return s;
+    E.mark(stage0 + 1, st);
+    if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(L.P) * items, static_cast<uint32_t>(p->wc_tuples), off,
+                                   tiles, ctr + (side == 0 ? CTR_BTILE : CTR_PTILE), status, st)) != PJ_OK)
+        return s;
+    E.mark(stage0 + 2, st);
+    return launch_scatter<K>(keys, n, chunk, items, f, L.P, p->wc_tuples, off, tuples, cap, status, st);
+}
 
 template <typename K>
 pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uint8_t* ws, int32_t* out_b,
@@ -379,44 +488,33 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
         for (int i = 0; i < PJ_NUM_STAGES; ++i) E.mark(i, st);
         return PJ_OK;
     }
-
-    const DigitFn f = digit_fn(p->digit_mode, 0, p->bits1, 0);
     pj_status s;
-    for (int side = 0; side < 2; ++side) {
-        const K* keys = static_cast<const K*>(side == 0 ? d->build_keys : d->probe_keys);
-        const int64_t n = side == 0 ? d->n_build : d->n_probe;
-        const int64_t chunk = side == 0 ? L.b_chunk : L.p_chunk;
-        const int items = side == 0 ? L.b_items : L.p_items;
-        uint32_t* counts = reinterpret_cast<uint32_t*>(ws + (side == 0 ? L.b_counts : L.p_counts));
-        int32_t* tot = reinterpret_cast<int32_t*>(ws + (side == 0 ? L.b_tot : L.p_tot));
-        int64_t* off = reinterpret_cast<int64_t*>(ws + (side == 0 ? L.b_off : L.p_off));
-        uint64_t* tiles = reinterpret_cast<uint64_t*>(ws + (side == 0 ? L.b_tiles : L.p_tiles));
-        uint32_t* tuples = reinterpret_cast<uint32_t*>(ws + (side == 0 ? L.b_tuples : L.p_tuples));
-        const int64_t cap = side == 0 ? L.b_cap : L.p_cap;
-        const int st0 = side == 0 ? PJ_STAGE_BUILD_HIST : PJ_STAGE_PROBE_HIST;
-        E.mark(st0, st);
-        if ((s = launch_hist<K>(keys, n, chunk, items, f, L.P, counts, tot, status, st)) != PJ_OK) return s;
-        E.mark(st0 + 1, st);
-        if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(L.P) * items, static_cast<uint32_t>(sc_w<K>()),
-                                       off, tiles, ctr + (side == 0 ? CTR_BTILE : CTR_PTILE), status, st)) != PJ_OK)
-            return s;
-        E.mark(st0 + 2, st);
-        if ((s = launch_scatter<K>(keys, n, chunk, items, f, L.P, off, tuples, cap, status, st)) != PJ_OK) return s;
-    }
+    if ((s = partition_column<K>(static_cast<const K*>(d->build_keys), d->n_build, p, L, 0, ws,
+                                 reinterpret_cast<uint32_t*>(ws + L.b_tuples), L.b_cap, E, PJ_STAGE_BUILD_HIST,
+                                 st)) != PJ_OK)
+        return s;
+    if ((s = partition_column<K>(static_cast<const K*>(d->probe_keys), d->n_probe, p, L, 1, ws,
+                                 reinterpret_cast<uint32_t*>(ws + L.p_tuples), L.p_cap, E, PJ_STAGE_PROBE_HIST,
+                                 st)) != PJ_OK)
+        return s;
     E.mark(PJ_STAGE_JOIN_PLAN, st);
 
-    const int cap_per_table = std::max(1, static_cast<int>(p->table_slots * p->max_fill));
+    const int cap_tuples = table_tuples(p);
     const bool hash_split = p->split_mode == PJ_SPLIT_HASH;
+    const int position_chunk = std::max(16, cap_tuples / 16 * 16);
     join_items_kernel<<<(L.P + 255) / 256, 256, 0, st>>>(
         reinterpret_cast<int64_t*>(ws + L.b_off), reinterpret_cast<int64_t*>(ws + L.p_off), L.b_items, L.p_items,
-        L.P, reinterpret_cast<int32_t*>(ws + L.b_tot), reinterpret_cast<int32_t*>(ws + L.p_tot), cap_per_table,
-        p->probe_chunk, hash_split ? 1 : 0, MAX_SPLIT_LOG2, reinterpret_cast<int32_t*>(ws + L.split),
-        reinterpret_cast<int64_t*>(ws + L.items), status);
+        L.P, reinterpret_cast<int32_t*>(ws + L.b_tot), reinterpret_cast<int32_t*>(ws + L.p_tot),
+        hash_split ? cap_tuples : position_chunk, p->probe_chunk, hash_split ? 1 : 0, MAX_SPLIT_LOG2,
+        reinterpret_cast<int32_t*>(ws + L.split), reinterpret_cast<int64_t*>(ws + L.items), status);
     PJ_CUDA(cudaGetLastError());
     if ((s = launch_scan<int64_t>(reinterpret_cast<int64_t*>(ws + L.items), L.P, 1u,
                                   reinterpret_cast<int64_t*>(ws + L.item_off), reinterpret_cast<uint64_t*>(ws + L.i_tiles),
                                   ctr + CTR_ITILE, status, st)) != PJ_OK)
         return s;
+    items_expand_kernel<<<L.P, 256, 0, st>>>(reinterpret_cast<int64_t*>(ws + L.item_off), L.P,
+                                             reinterpret_cast<int32_t*>(ws + L.item_part), L.max_items, status);
+    PJ_CUDA(cudaGetLastError());
 
     JoinArgs a{};
     a.build_tuples = reinterpret_cast<const uint32_t*>(ws + L.b_tuples);
@@ -427,19 +525,28 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     a.p_items = L.p_items;
     a.P = L.P;
     a.digit_bits = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 + p->bits2 : 0;
-    a.split_log2 = reinterpret_cast<const int32_t*>(ws + L.split);
+    a.split = reinterpret_cast<const int32_t*>(ws + L.split);
     a.item_off = reinterpret_cast<const int64_t*>(ws + L.item_off);
+    a.item_part = reinterpret_cast<const int32_t*>(ws + L.item_part);
+    a.max_items = L.max_items;
     a.queue = ctr + CTR_QUEUE;
-    a.table_slots = p->table_slots;
+    a.cap = p->table_capacity;
+    a.nb_log2 = bucket_nb_log2(p->table_capacity);
     a.probe_chunk = p->probe_chunk;
-    a.position_chunk = std::max(16, cap_per_table / 16 * 16);
+    a.position_chunk = position_chunk;
     a.out_build = out_b;
     a.out_probe = out_p;
     a.capacity = capacity;
     a.count = reinterpret_cast<unsigned long long*>(count);
     a.status = status;
+    a.cta_q = reinterpret_cast<int64_t*>(ws + L.cta_q);
+    a.cta_last = reinterpret_cast<int64_t*>(ws + L.cta_last);
+    a.seg = reinterpret_cast<int64_t*>(ws + L.seg);
+    a.over_build = reinterpret_cast<int32_t*>(ws + L.over_b);
+    a.over_probe = reinterpret_cast<int32_t*>(ws + L.over_p);
+    a.over_cap = L.over_cap;
     E.mark(PJ_STAGE_JOIN, st);
-    s = launch_join<K>(a, d->unique_build_keys != 0, hash_split, p->slot_mode == PJ_SLOT_REF, st);
+    s = launch_join<K>(a, p->table_mode, d->unique_build_keys != 0, hash_split, p->slot_mode == PJ_SLOT_REF, st);
     E.mark(PJ_STAGE_TOTAL, st);
     return s;
 }
@@ -452,6 +559,44 @@ pj_status resolve_plan(const pj_join_desc* d, const pj_plan* in, pj_plan* out)
         if (s != PJ_OK) return s;
     }
     return check_plan(d, out);
+}
+
+pj_status check_ws(const pj_join_desc* d, const pj_plan* p, void* ws, size_t ws_bytes, Layout* L)
+{
+    *L = make_layout(d, p);
+    if (!ws || (reinterpret_cast<uintptr_t>(ws) & 255u) || ws_bytes < L->total) return PJ_ERR_WORKSPACE;
+    return PJ_OK;
+}
+
+pj_status check_inputs(const pj_join_desc* d)
+{
+    if (d->n_build > 0 && !aligned16(d->build_keys)) return PJ_ERR_ALIGNMENT;
+    if (d->n_probe > 0 && !aligned16(d->probe_keys)) return PJ_ERR_ALIGNMENT;
+    return PJ_OK;
+}
+
+pj_status check_output(const pj_output* out)
+{
+    if (!out || !out->count || out->capacity < 0) return PJ_ERR_INVALID;
+    if (out->capacity > 0 && (!out->build_row || !out->probe_row)) return PJ_ERR_INVALID;
+    return PJ_OK;
+}
+
+pj_status prepare(const pj_join_desc* d, const pj_plan* plan, void* ws, size_t ws_bytes, pj_plan* p, Layout* L)
+{
+    if (!valid_desc(d)) return PJ_ERR_INVALID;
+    pj_status s = resolve_plan(d, plan, p);
+    if (s != PJ_OK) return s;
+    if ((s = check_inputs(d)) != PJ_OK) return s;
+    return check_ws(d, p, ws, ws_bytes, L);
+}
+
+pj_status dispatch_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, void* ws, int32_t* ob, int32_t* op,
+                        int64_t cap, int64_t* count, cudaStream_t st, const StageEvents& E)
+{
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    if (d->key_bytes == 4) return run_join<int32_t>(d, p, L, w, ob, op, cap, count, st, E);
+    return run_join<int64_t>(d, p, L, w, ob, op, cap, count, st, E);
 }
 
 }  // namespace
@@ -475,7 +620,7 @@ const char* pj_status_string(pj_status s)
     return "unknown status";
 }
 
-const char* pj_version(void) { return "partitioned_join_b200 0.1 (sm_100a)"; }
+const char* pj_version(void) { return "partitioned_join_b200 0.2 (sm_100a)"; }
 
 pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
 {
@@ -483,19 +628,29 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     std::memset(p, 0, sizeof(*p));
     p->passes = 1;
     p->digit_mode = PJ_DIGIT_HASH;
+    p->table_mode = PJ_TABLE_BUCKET;
     p->slot_mode = PJ_SLOT_FAST;
     p->split_mode = d->unique_build_keys ? PJ_SPLIT_HASH : PJ_SPLIT_POSITION;
     p->max_fill = 0.5f;  // HASH_TABLE_OCC, hash_join_kernels.cuh:21
-    p->table_slots = d->key_bytes == 4 ? 16384 : 8192;
-    p->table_slots = std::min(p->table_slots, max_table_slots(d->key_bytes));
-    p->join_threads = JN_THREADS;
-    p->scatter_threads = SC_THREADS;
-    p->scatter_ctas_per_sm = 1;
+    p->table_capacity = max_table_capacity(d->key_bytes, p->table_mode);
     p->probe_chunk = 1 << 16;
-    const int64_t cap = static_cast<int64_t>(p->table_slots * p->max_fill);
-    const int want = ilog2_ceil(std::max<int64_t>(1, (d->n_build + cap - 1) / cap));
-    p->bits1 = std::min(want, max_one_pass_bits(d->key_bytes));
-    p->bits2 = 0;
+    p->scatter_ctas_per_sm = 1;
+    p->hist_split = 2;
+    // Fewest partitions whose expected build side fills at most 7/8 of a table.
+    const int64_t target = std::max<int64_t>(1, p->table_capacity - p->table_capacity / 8);
+    int bits = ilog2_ceil(std::max<int64_t>(1, (d->n_build + target - 1) / target));
+    // Widest write-combining buffer that the shared memory allows at that fan-out.
+    auto pick_w = [&](int b) {
+        for (int W : {8, 4})
+            if (sector_wc(d->key_bytes, W) && scatter_smem(d->key_bytes, W, 1 << b) <= smem_limit() &&
+                (W <= 4 || b <= 8))
+                return W;
+        return 0;
+    };
+    while (bits > 0 && pick_w(bits) == 0) --bits;  // beyond one pass: hash splits absorb the rest
+    p->bits1 = bits;
+    p->wc_tuples = pick_w(bits);
+    if (p->wc_tuples == 0) p->wc_tuples = d->key_bytes == 4 ? 4 : 8;
     return PJ_OK;
 }
 
@@ -509,58 +664,50 @@ pj_status pj_workspace_size(const pj_join_desc* d, const pj_plan* plan, size_t* 
     return PJ_OK;
 }
 
-static pj_status check_ws(const pj_join_desc* d, const pj_plan* p, void* ws, size_t ws_bytes, Layout* L)
-{
-    *L = make_layout(d, p);
-    if (!ws || (reinterpret_cast<uintptr_t>(ws) & 255u) || ws_bytes < L->total) return PJ_ERR_WORKSPACE;
-    return PJ_OK;
-}
-
-static pj_status check_inputs(const pj_join_desc* d)
-{
-    if (d->n_build > 0 && !aligned16(d->build_keys)) return PJ_ERR_ALIGNMENT;
-    if (d->n_probe > 0 && !aligned16(d->probe_keys)) return PJ_ERR_ALIGNMENT;
-    return PJ_OK;
-}
-
 pj_status pj_inner_join(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws, size_t ws_bytes,
                         pj_stream stream)
 {
-    if (!valid_desc(d) || !out || !out->count || out->capacity < 0) return PJ_ERR_INVALID;
-    if (out->capacity > 0 && (!out->build_row || !out->probe_row)) return PJ_ERR_INVALID;
-    pj_plan p;
-    pj_status s = resolve_plan(d, plan, &p);
+    pj_status s = check_output(out);
     if (s != PJ_OK) return s;
-    if ((s = check_inputs(d)) != PJ_OK) return s;
+    pj_plan p;
     Layout L;
-    if ((s = check_ws(d, &p, ws, ws_bytes, &L)) != PJ_OK) return s;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint8_t* w = static_cast<uint8_t*>(ws);
-    if (d->key_bytes == 4) return run_join<int32_t>(d, &p, L, w, out->build_row, out->probe_row, out->capacity, out->count, st);
-    return run_join<int64_t>(d, &p, L, w, out->build_row, out->probe_row, out->capacity, out->count, st);
+    if ((s = prepare(d, plan, ws, ws_bytes, &p, &L)) != PJ_OK) return s;
+    return dispatch_join(d, &p, L, ws, out->build_row, out->probe_row, out->capacity, out->count,
+                         static_cast<cudaStream_t>(stream), StageEvents());
+}
+
+pj_status pj_inner_join_events(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws,
+                               size_t ws_bytes, pj_stream stream, void* const* events)
+{
+    pj_status s = check_output(out);
+    if (s != PJ_OK) return s;
+    if (!events) return PJ_ERR_INVALID;
+    for (int i = 0; i < PJ_NUM_STAGES; ++i)
+        if (!events[i]) return PJ_ERR_INVALID;
+    pj_plan p;
+    Layout L;
+    if ((s = prepare(d, plan, ws, ws_bytes, &p, &L)) != PJ_OK) return s;
+    StageEvents E;
+    E.ev = reinterpret_cast<cudaEvent_t*>(const_cast<void**>(events));
+    return dispatch_join(d, &p, L, ws, out->build_row, out->probe_row, out->capacity, out->count,
+                         static_cast<cudaStream_t>(stream), E);
 }
 
 pj_status pj_inner_join_timed(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws,
                               size_t ws_bytes, pj_stream stream, float* stage_ms)
 {
-    if (!valid_desc(d) || !out || !out->count || out->capacity < 0 || !stage_ms) return PJ_ERR_INVALID;
-    if (out->capacity > 0 && (!out->build_row || !out->probe_row)) return PJ_ERR_INVALID;
-    pj_plan p;
-    pj_status s = resolve_plan(d, plan, &p);
+    pj_status s = check_output(out);
     if (s != PJ_OK) return s;
-    if ((s = check_inputs(d)) != PJ_OK) return s;
+    if (!stage_ms) return PJ_ERR_INVALID;
+    pj_plan p;
     Layout L;
-    if ((s = check_ws(d, &p, ws, ws_bytes, &L)) != PJ_OK) return s;
+    if ((s = prepare(d, plan, ws, ws_bytes, &p, &L)) != PJ_OK) return s;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaEvent_t ev[PJ_NUM_STAGES];
     for (int i = 0; i < PJ_NUM_STAGES; ++i) PJ_CUDA(cudaEventCreate(&ev[i]));
     StageEvents E;
     E.ev = ev;
-    uint8_t* w = static_cast<uint8_t*>(ws);
-    if (d->key_bytes == 4)
-        s = run_join<int32_t>(d, &p, L, w, out->build_row, out->probe_row, out->capacity, out->count, st, E);
-    else
-        s = run_join<int64_t>(d, &p, L, w, out->build_row, out->probe_row, out->capacity, out->count, st, E);
+    s = dispatch_join(d, &p, L, ws, out->build_row, out->probe_row, out->capacity, out->count, st, E);
     cudaError_t e = cudaStreamSynchronize(st);
     if (s == PJ_OK && e == cudaSuccess) {
         for (int i = 0; i + 1 < PJ_NUM_STAGES; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
@@ -574,43 +721,17 @@ pj_status pj_inner_join_timed(const pj_join_desc* d, const pj_plan* plan, pj_out
     return s;
 }
 
-pj_status pj_inner_join_events(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws,
-                               size_t ws_bytes, pj_stream stream, void* const* events)
-{
-    if (!valid_desc(d) || !out || !out->count || out->capacity < 0 || !events) return PJ_ERR_INVALID;
-    if (out->capacity > 0 && (!out->build_row || !out->probe_row)) return PJ_ERR_INVALID;
-    for (int i = 0; i < PJ_NUM_STAGES; ++i)
-        if (!events[i]) return PJ_ERR_INVALID;
-    pj_plan p;
-    pj_status s = resolve_plan(d, plan, &p);
-    if (s != PJ_OK) return s;
-    if ((s = check_inputs(d)) != PJ_OK) return s;
-    Layout L;
-    if ((s = check_ws(d, &p, ws, ws_bytes, &L)) != PJ_OK) return s;
-    StageEvents E;
-    E.ev = reinterpret_cast<cudaEvent_t*>(const_cast<void**>(events));
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint8_t* w = static_cast<uint8_t*>(ws);
-    if (d->key_bytes == 4)
-        return run_join<int32_t>(d, &p, L, w, out->build_row, out->probe_row, out->capacity, out->count, st, E);
-    return run_join<int64_t>(d, &p, L, w, out->build_row, out->probe_row, out->capacity, out->count, st, E);
-}
-
 pj_status pj_join_count(const pj_join_desc* d, const pj_plan* plan, int64_t* count_dev, void* ws, size_t ws_bytes,
                         pj_stream stream)
 {
-    if (!valid_desc(d) || !count_dev) return PJ_ERR_INVALID;
+    if (!count_dev) return PJ_ERR_INVALID;
     pj_plan p;
-    pj_status s = resolve_plan(d, plan, &p);
-    if (s != PJ_OK) return s;
-    if ((s = check_inputs(d)) != PJ_OK) return s;
     Layout L;
-    if ((s = check_ws(d, &p, ws, ws_bytes, &L)) != PJ_OK) return s;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint8_t* w = static_cast<uint8_t*>(ws);
-    // capacity 0: the join kernel counts every match and writes none
-    if (d->key_bytes == 4) return run_join<int32_t>(d, &p, L, w, nullptr, nullptr, 0, count_dev, st);
-    return run_join<int64_t>(d, &p, L, w, nullptr, nullptr, 0, count_dev, st);
+    pj_status s = prepare(d, plan, ws, ws_bytes, &p, &L);
+    if (s != PJ_OK) return s;
+    // no output columns: the join counts every match and writes none
+    return dispatch_join(d, &p, L, ws, nullptr, nullptr, 0, count_dev, static_cast<cudaStream_t>(stream),
+                         StageEvents());
 }
 
 pj_status pj_check(void* ws, pj_stream stream)
@@ -698,7 +819,8 @@ pj_status pj_radix_histogram(const void* keys, int64_t n, int32_t key_bytes, int
 pj_status pj_partitioned_capacity(int64_t n, int32_t key_bytes, const pj_plan* plan, int64_t* tuples)
 {
     if (n < 0 || n > INT32_MAX || (key_bytes != 4 && key_bytes != 8) || !plan || !tuples) return PJ_ERR_INVALID;
-    *tuples = part_capacity(n, key_bytes, 1 << plan->bits1, scatter_items(plan));
+    if (!valid_wc(key_bytes, plan->wc_tuples)) return PJ_ERR_INVALID;
+    *tuples = part_capacity(n, 1 << plan->bits1, scatter_items(plan), plan->wc_tuples);
     return PJ_OK;
 }
 
@@ -710,9 +832,7 @@ pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_
         return PJ_ERR_INVALID;
     pj_join_desc d{};
     d.build_keys = keys;
-    d.probe_keys = keys;
     d.n_build = n;
-    d.n_probe = 0;
     d.key_bytes = key_bytes;
     d.unique_build_keys = 1;
     pj_status s = check_plan(&d, plan);
@@ -723,20 +843,13 @@ pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_
     if ((s = check_ws(&d, plan, ws, ws_bytes, &L)) != PJ_OK) return s;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     uint8_t* w = static_cast<uint8_t*>(ws);
-    uint32_t* status = reinterpret_cast<uint32_t*>(w + L.status);
-    uint32_t* ctr = reinterpret_cast<uint32_t*>(w + L.counters);
     PJ_CUDA(cudaMemsetAsync(w, 0, L.ctrl_end, st));
-    const DigitFn f = digit_fn(plan->digit_mode, 0, plan->bits1, 0);
     if (key_bytes == 4)
-        s = partition_side<int32_t>(static_cast<const int32_t*>(keys), n, L.b_chunk, L.b_items, f, L.P,
-                                    reinterpret_cast<uint32_t*>(w + L.b_counts), reinterpret_cast<int32_t*>(w + L.b_tot),
-                                    reinterpret_cast<int64_t*>(w + L.b_off), reinterpret_cast<uint64_t*>(w + L.b_tiles),
-                                    ctr + CTR_BTILE, static_cast<uint32_t*>(tuples), L.b_cap, status, st);
+        s = partition_column<int32_t>(static_cast<const int32_t*>(keys), n, plan, L, 0, w, static_cast<uint32_t*>(tuples),
+                                      L.b_cap, StageEvents(), 0, st);
     else
-        s = partition_side<int64_t>(static_cast<const int64_t*>(keys), n, L.b_chunk, L.b_items, f, L.P,
-                                    reinterpret_cast<uint32_t*>(w + L.b_counts), reinterpret_cast<int32_t*>(w + L.b_tot),
-                                    reinterpret_cast<int64_t*>(w + L.b_off), reinterpret_cast<uint64_t*>(w + L.b_tiles),
-                                    ctr + CTR_BTILE, static_cast<uint32_t*>(tuples), L.b_cap, status, st);
+        s = partition_column<int64_t>(static_cast<const int64_t*>(keys), n, plan, L, 0, w, static_cast<uint32_t*>(tuples),
+                                      L.b_cap, StageEvents(), 0, st);
     if (s != PJ_OK) return s;
     partition_bounds_kernel<<<(L.P + 1 + 255) / 256, 256, 0, st>>>(reinterpret_cast<int64_t*>(w + L.b_off), L.b_items,
                                                                    L.P, offsets);
@@ -755,29 +868,40 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
         return PJ_OK;
     }
     if ((s = check_inputs(d)) != PJ_OK) return s;
-    // The histogram goes into the workspace's build-count area, which every
-    // plan of this join has room for (P x items >= P).
     Layout L;
     if ((s = check_ws(d, &p, ws, ws_bytes, &L)) != PJ_OK) return s;
     const int P = 1 << p.bits1;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Histograms of the build keys under both digit sources, in the
+    // workspace's count area (P x items >= 2P words).
     int32_t* hist = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(ws) + L.b_counts);
-    if ((s = pj_radix_histogram(d->build_keys, d->n_build, d->key_bytes, p.digit_mode, p.bits1, 0, 0, hist, stream)) != PJ_OK)
+    if ((s = pj_radix_histogram(d->build_keys, d->n_build, d->key_bytes, PJ_DIGIT_RAW, p.bits1, 0, 0, hist, stream)) !=
+        PJ_OK)
         return s;
-    int32_t* host = new int32_t[P];
-    cudaError_t e = cudaMemcpyAsync(host, hist, sizeof(int32_t) * P, cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream));
-    if (e == cudaSuccess) e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if ((s = pj_radix_histogram(d->build_keys, d->n_build, d->key_bytes, PJ_DIGIT_HASH, p.bits1, 0, 0, hist + P,
+                                stream)) != PJ_OK)
+        return s;
+    int32_t* host = new int32_t[2 * static_cast<size_t>(P)];
+    cudaError_t e = cudaMemcpyAsync(host, hist, sizeof(int32_t) * 2 * P, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         delete[] host;
         last_cuda_error() = e;
         return PJ_ERR_CUDA;
     }
-    int64_t mx = 0;
-    for (int i = 0; i < P; ++i) mx = std::max<int64_t>(mx, host[i]);
+    int64_t raw_max = 0, hash_max = 0;
+    for (int i = 0; i < P; ++i) {
+        raw_max = std::max<int64_t>(raw_max, host[i]);
+        hash_max = std::max<int64_t>(hash_max, host[P + i]);
+    }
     delete[] host;
-    const int64_t cap = static_cast<int64_t>(p.table_slots * p.max_fill);
+    // Raw key bits are free to compute: keep them (the reference's digits)
+    // when their largest partition is no worse than the hashed one's.
+    p.digit_mode = raw_max <= hash_max ? PJ_DIGIT_RAW : PJ_DIGIT_HASH;
+    const int64_t mx = std::min(raw_max, hash_max);
+    const int64_t cap = table_tuples(&p);
     // Hash splits cannot separate repeated keys: a partition beyond what
-    // 2^MAX_SPLIT_LOG2 tables hold (duplicates) falls back to the
-    // reference's position split.
+    // 2^MAX_SPLIT_LOG2 tables hold (duplicates) takes the position split.
     if (mx > cap * (int64_t(1) << MAX_SPLIT_LOG2) / 2) p.split_mode = PJ_SPLIT_POSITION;
     *plan = p;
     return PJ_OK;

@@ -4,39 +4,47 @@
 // work split of handle_skewed_data (skewed_data_handler.cuh:21-91) and the
 // launch of shared_memory_hash_join (partitioned_join.cuh:178-251).
 //
-// Work items.  Partition p with b build and q probe tuples (padded ranges
-// from the scatter) becomes S_p x K_p items: S_p splits the build side so
-// that each piece fits one table (by hash bits, or by position as the
-// reference does), K_p = ceil(q / probe_chunk) splits the probe side (the
-// reference has no probe split, so one CTA walks a hot partition's whole
-// probe run).  Items are numbered partition-major, then probe chunk, then
-// build split, so the CTAs that share a probe chunk run side by side and
-// read it from L2.  A persistent grid claims items through an atomic
-// counter.
+// Work items.  Partition p with b build and q probe tuples becomes S_p x K_p
+// items: S_p splits the build side so that every piece fits one table (by
+// hash bits -- each probe row then visits one table -- or by position, the
+// reference's split, when repeated keys defeat hashing), K_p =
+// ceil(q / probe_chunk) splits the probe side (the reference has no probe
+// split, so one CTA walks a hot partition's whole probe run).  Items are
+// numbered partition-major, then probe chunk, then build piece, so CTAs that
+// share data run side by side.  A persistent grid claims items through an
+// atomic counter (the next claim is issued while the current item runs).
 //
-// Table.  Open addressing with linear probing, table_slots slots of
-// {key, row}; row == -1 marks an empty slot, so every key value (the
-// reference's -1 sentinel included) joins.  Inserts claim a slot with a CAS
-// on the row word.  The slot of a key is PJ_SLOT_FAST (multiply-high of the
-// hash bits that digits and splits did not consume) or PJ_SLOT_REF
-// (abs((int)h % T), hash_join_kernels.cuh:100-101).
+// Tables (shared memory).
+//   BUCKET (default): the piece's build tuples sorted by bucket = low hash
+//     bits, plus an array of bucket ends (16-bit, two per word).  Built by a
+//     counting sort: count pass, block scan, place pass.  8 bytes a tuple for
+//     4-byte keys, so one CTA holds ~18 K tuples.
+//   OPEN: the reference's layout -- open addressing with linear probing,
+//     fill <= 0.5 (HASH_TABLE_OCC, hash_join_kernels.cuh:21), slot
+//     abs((int)h % T) (:100-101) or a multiply-high of unused hash bits;
+//     a CAS on the row word claims a slot, row == -1 marks it empty, so every
+//     key value (the reference's -1 sentinel included) joins.
 //
-// Output.  Matches are appended to a shared-memory buffer with one shared
-// atomic per warp (ballot + popc); when the buffer passes its high-water
-// mark the CTA reserves room in the output with ONE global atomicAdd and
-// copies the buffer out coalesced (the reference's write_back_buffer,
-// hash_join_kernels.cuh:150-199, does a global atomic per overflowing match).
+// Output.  Probing has no block-wide barrier: each warp stages its matches
+// in a small shared buffer (ballot/scan compaction), reserves their
+// positions with one shared atomic on the CTA's entry counter and copies
+// them out coalesced.  A CTA claims output space from the global counter
+// OUT_CHUNK entries at a time, so global atomics are rare (the reference's
+// write_back_buffer, hash_join_kernels.cuh:150-199, does one per match past
+// its buffer).  Each CTA's last chunk is only partly used; a fix-up pass
+// (join_fixup_plan_kernel / join_fixup_move_kernel) moves the entries above
+// the true total into those gaps, so the output is dense.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "pj_bulk.cuh"
 #include "pj_device.cuh"
 
 namespace pj {
 
 constexpr uint32_t EMPTY_ROW = 0xffffffffu;
+enum : int { TABLE_BUCKET = 0, TABLE_OPEN = 1 };
 
 struct JoinArgs {
     const uint32_t* build_tuples;
@@ -47,17 +55,26 @@ struct JoinArgs {
     int32_t p_items;
     int32_t P;
     int32_t digit_bits;         // top hash bits consumed by partition digits (HASH digits), else 0
-    const int32_t* split_log2;  // per partition: log2 S_p (hash split) or S_p (position split)
+    const int32_t* split;       // per partition: log2 S_p (hash split) or S_p (position split)
     const int64_t* item_off;    // exclusive scan of items per partition, P+1 entries
+    const int32_t* item_part;   // partition of every item
+    int64_t max_items;
     uint32_t* queue;            // item counter (zeroed)
-    int32_t table_slots;
+    int32_t cap;                // build tuples one table holds (BUCKET) / slots (OPEN)
+    int32_t nb_log2;            // BUCKET: log2 of the bucket count
     int32_t probe_chunk;        // tuples
     int32_t position_chunk;     // build tuples per position split piece
-    int32_t* out_build;
+    int32_t* out_build;         // nullptr: count only
     int32_t* out_probe;
     int64_t capacity;
-    unsigned long long* count;  // device int64 match counter
+    unsigned long long* count;  // device int64: chunk reservations, then the match count
     uint32_t* status;
+    int64_t* cta_q;             // per CTA: entries produced
+    int64_t* cta_last;          // per CTA: base of its last output chunk (-1: none)
+    int32_t* over_build;        // reserved positions >= capacity land here
+    int32_t* over_probe;
+    int64_t over_cap;
+    int64_t* seg;               // fix-up segments
 };
 
 // Items per partition (S_p x K_p) and the split of partition p.
@@ -77,12 +94,15 @@ __global__ void join_items_kernel(const int64_t* __restrict__ build_off, const i
     if (bc > 0 && pc > 0) {
         int64_t S;
         if (hash_split) {
+            // hash pieces are only about equal: aim each at 15/16 of a table
+            const int64_t target = cap_per_table - cap_per_table / 16;
             int lg = 0;
-            while (lg < max_split_log2 && (bc + (1ll << lg) - 1) / (1ll << lg) > cap_per_table) ++lg;
+            while (lg < max_split_log2 && (bc + (1ll << lg) - 1) / (1ll << lg) > target) ++lg;
             split = lg;
             S = 1ll << lg;
         } else {
-            S = (bc + cap_per_table - 1) / cap_per_table;
+            const int64_t brange = build_off[static_cast<int64_t>(p + 1) * b_items] - build_off[static_cast<int64_t>(p) * b_items];
+            S = (brange + cap_per_table - 1) / cap_per_table;
             if (S < 1) S = 1;
             split = static_cast<int32_t>(S);
         }
@@ -93,164 +113,303 @@ __global__ void join_items_kernel(const int64_t* __restrict__ build_off, const i
     items_out[p] = items;
 }
 
-template <typename K> struct TableSlot;
-
-// 4-byte keys: one 8-byte slot {key, row} -> one shared load per step.
-template <> struct TableSlot<int32_t> {
-    static constexpr int BYTES = 8;
-    uint2* s;
-    __device__ __forceinline__ void bind(uint8_t* base, int T) { (void)T; s = reinterpret_cast<uint2*>(base); }
-    __device__ __forceinline__ void clear(int i) { s[i] = make_uint2(0u, EMPTY_ROW); }
-    __device__ __forceinline__ bool try_claim(int i, int32_t key, int32_t row)
-    {
-        if (atomicCAS(&s[i].y, EMPTY_ROW, static_cast<uint32_t>(row)) == EMPTY_ROW) {
-            s[i].x = static_cast<uint32_t>(key);
-            return true;
-        }
-        return false;
+// item_part[item_off[p] + k] = p for k < items of p.
+__global__ void items_expand_kernel(const int64_t* __restrict__ item_off, int32_t P, int32_t* __restrict__ item_part,
+                                    int64_t max_items, uint32_t* __restrict__ status)
+{
+    const int p = blockIdx.x;
+    if (p >= P) return;
+    const int64_t a = item_off[p], b = item_off[p + 1];
+    if (b > max_items) {
+        if (threadIdx.x == 0) raise_status(status, ST_OVERFLOW);
+        return;
     }
-    // returns row, or EMPTY_ROW; sets hit if the key matches
-    __device__ __forceinline__ uint32_t look(int i, int32_t key, bool& hit) const
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) item_part[i] = p;
+}
+
+// ---------------------------------------------------------------------------
+// Tuple access: a probe/build tuple gives (hash, comparable key, row).
+// 4-byte keys: the stored word 0 is murmur(key), a bijection, so the hash is
+// the key.  8-byte keys: the key is stored, the hash recomputed.
+template <typename K> struct TupleView;
+
+template <> struct TupleView<int32_t> {
+    static constexpr int WORDS = 2;
+    using Cmp = uint32_t;
+    __device__ __forceinline__ static void load(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key, int32_t& row)
     {
-        const uint2 v = s[i];
-        hit = v.y != EMPTY_ROW && static_cast<int32_t>(v.x) == key;
-        return v.y;
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(base) + i);
+        h = v.x;
+        key = v.x;
+        row = static_cast<int32_t>(v.y);
     }
 };
 
-// 8-byte keys: keys[T] then rows[T] (12 bytes a slot).
-template <> struct TableSlot<int64_t> {
-    static constexpr int BYTES = 12;
-    unsigned long long* k;
-    uint32_t* r;
-    __device__ __forceinline__ void bind(uint8_t* base, int T)
+template <> struct TupleView<int64_t> {
+    static constexpr int WORDS = 3;
+    using Cmp = unsigned long long;
+    __device__ __forceinline__ static void load(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key, int32_t& row)
     {
-        k = reinterpret_cast<unsigned long long*>(base);
-        r = reinterpret_cast<uint32_t*>(base + static_cast<size_t>(T) * 8);
-    }
-    __device__ __forceinline__ void clear(int i) { r[i] = EMPTY_ROW; }
-    __device__ __forceinline__ bool try_claim(int i, int64_t key, int32_t row)
-    {
-        if (atomicCAS(&r[i], EMPTY_ROW, static_cast<uint32_t>(row)) == EMPTY_ROW) {
-            k[i] = static_cast<unsigned long long>(key);
-            return true;
-        }
-        return false;
-    }
-    __device__ __forceinline__ uint32_t look(int i, int64_t key, bool& hit) const
-    {
-        const uint32_t row = r[i];
-        hit = row != EMPTY_ROW && static_cast<int64_t>(k[i]) == key;
-        return row;
+        const uint32_t* p = base + 3 * i;
+        const uint32_t lo = __ldg(p), hi = __ldg(p + 1);
+        key = (static_cast<unsigned long long>(hi) << 32) | lo;
+        row = static_cast<int32_t>(__ldg(p + 2));
+        h = hash_key(static_cast<int64_t>(key));
     }
 };
 
-template <typename K>
-__device__ __forceinline__ void smem_tuple(const uint8_t* stage, int j, K& key, int32_t& row);
+// Entry of a BUCKET table.
+template <typename K> struct Entry;
+template <> struct Entry<int32_t> {
+    static constexpr int BYTES = 8;  // {hash/key, row}
+    __device__ __forceinline__ static void put(uint8_t* t, int i, uint32_t key, int32_t row)
+    {
+        reinterpret_cast<uint2*>(t)[i] = make_uint2(key, static_cast<uint32_t>(row));
+    }
+    __device__ __forceinline__ static void get(const uint8_t* t, int i, uint32_t& key, uint32_t& row)
+    {
+        const uint2 v = reinterpret_cast<const uint2*>(t)[i];
+        key = v.x;
+        row = v.y;
+    }
+};
+template <> struct Entry<int64_t> {
+    static constexpr int BYTES = 12;  // {lo, hi, row}
+    __device__ __forceinline__ static void put(uint8_t* t, int i, unsigned long long key, int32_t row)
+    {
+        uint32_t* w = reinterpret_cast<uint32_t*>(t) + 3 * i;
+        w[0] = static_cast<uint32_t>(key);
+        w[1] = static_cast<uint32_t>(key >> 32);
+        w[2] = static_cast<uint32_t>(row);
+    }
+    __device__ __forceinline__ static void get(const uint8_t* t, int i, unsigned long long& key, uint32_t& row)
+    {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(t) + 3 * i;
+        key = (static_cast<unsigned long long>(w[1]) << 32) | w[0];
+        row = w[2];
+    }
+};
 
-template <>
-__device__ __forceinline__ void smem_tuple<int32_t>(const uint8_t* stage, int j, int32_t& key, int32_t& row)
+// Asynchronous prefetch of a byte range into L2 (the bulk-copy engine's
+// prefetch form): 16-byte aligned start, issued in 64 KB pieces.
+__device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes)
 {
-    const uint2 v = reinterpret_cast<const uint2*>(stage)[j];
-    key = static_cast<int32_t>(v.x);
-    row = static_cast<int32_t>(v.y);
+    const uint8_t* c = static_cast<const uint8_t*>(p);
+    for (int64_t off = 0; off < bytes; off += 65536) {
+        const int64_t left = bytes - off;
+        const uint32_t n = static_cast<uint32_t>((left < 65536 ? left : 65536) & ~int64_t(15));
+        if (n) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + off), "r"(n) : "memory");
+    }
 }
 
-template <>
-__device__ __forceinline__ void smem_tuple<int64_t>(const uint8_t* stage, int j, int64_t& key, int32_t& row)
-{
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(stage) + 3 * j;
-    key = static_cast<int64_t>((static_cast<uint64_t>(w[1]) << 32) | w[0]);
-    row = static_cast<int32_t>(w[2]);
-}
+// Output geometry.
+constexpr int OUT_CHUNK = 8192;  // entries a CTA claims per global atomic
+constexpr int OUT_SLOTS = 16;    // chunk bases a CTA keeps in shared memory
+constexpr int JOIN_U = 4;        // probe tuples in flight per lane (and staged entries per lane)
+constexpr int JOIN_BU = 4;       // build tuples in flight per thread
 
-template <typename K, int THREADS, int OB, int NSTAGE, int STAGE_TUPLES>
+template <typename K, int TABLE>
 struct JoinSmem {
-    static constexpr int TB = TupleTraits<K>::WORDS * 4;
-    static constexpr int STAGE_BYTES = STAGE_TUPLES * TB;
-    static size_t bytes(int T)
+    // table bytes for capacity cap (BUCKET: tuples; OPEN: slots) and 2^nb_log2 buckets
+    __host__ __device__ static size_t entries_bytes(int cap)
     {
-        const size_t table = (static_cast<size_t>(T) * TableSlot<K>::BYTES + 127) & ~size_t(127);
-        return static_cast<size_t>(NSTAGE) * STAGE_BYTES + static_cast<size_t>(OB) * 8 + table;
+        const size_t e = TABLE == TABLE_OPEN ? (sizeof(K) == 4 ? 8 : 12) : Entry<K>::BYTES;
+        return (static_cast<size_t>(cap) * e + 127) & ~size_t(127);
+    }
+    __host__ __device__ static size_t table_bytes(int cap, int nb_log2)
+    {
+        size_t t = entries_bytes(cap);
+        if (TABLE == TABLE_BUCKET) t += ((static_cast<size_t>(1) << nb_log2) / 2) * 4;
+        return (t + 127) & ~size_t(127);
+    }
+    // plus per-warp staging of 32 * JOIN_U entries (build and probe rows)
+    __host__ __device__ static size_t bytes(int cap, int nb_log2, int threads)
+    {
+        return table_bytes(cap, nb_log2) + static_cast<size_t>(threads / 32) * 32 * JOIN_U * 8;
     }
 };
 
-__device__ __forceinline__ int upper_bound_i64(const int64_t* a, int n, int64_t x)
+// Exclusive scan, in place, of the 16-bit counts packed two per word in
+// w[0 .. nwords).  Totals stay below 65536.  Ends with __syncthreads().
+template <int THREADS>
+__device__ __forceinline__ void scan_u16_pairs(uint32_t* w, int nwords, uint32_t* s_warp)
 {
-    int lo = 0, hi = n;  // first index with a[i] > x
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (a[mid] <= x) lo = mid + 1; else hi = mid;
+    const int per = (nwords + THREADS - 1) / THREADS;
+    const int a = threadIdx.x * per;
+    const int b = a + per < nwords ? a + per : nwords;
+    uint32_t sum = 0;
+    for (int i = a; i < b; ++i) {
+        const uint32_t x = w[i];
+        sum += (x & 0xffffu) + (x >> 16);
     }
-    return lo;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t x = lane < THREADS / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < THREADS / 32) s_warp[lane] = x;
+    }
+    __syncthreads();
+    uint32_t run = incl - sum + (warp > 0 ? s_warp[warp - 1] : 0u);
+    for (int i = a; i < b; ++i) {
+        const uint32_t x = w[i];
+        const uint32_t c0 = x & 0xffffu, c1 = x >> 16;
+        w[i] = (run & 0xffffu) | ((run + c0) << 16);
+        run += c0 + c1;
+    }
+    __syncthreads();
 }
 
-template <typename K, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF, int THREADS, int OB, int NSTAGE,
-          int STAGE_TUPLES>
+template <typename K, int TABLE, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 {
-    using SM = JoinSmem<K, THREADS, OB, NSTAGE, STAGE_TUPLES>;
-    static_assert(STAGE_TUPLES % THREADS == 0, "a stage holds whole rounds");
-    static_assert(OB >= 2 * THREADS, "output buffer needs a round of headroom");
+    using TV = TupleView<K>;
+    using Cmp = typename TV::Cmp;
+    using E = Entry<K>;
+    using SM = JoinSmem<K, TABLE>;
+    constexpr int NWARPS = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto warp_id = [&]() { return warp; };
+    constexpr int U = JOIN_U;
+
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* stages = smem;
-    int32_t* ob_b = reinterpret_cast<int32_t*>(smem + NSTAGE * SM::STAGE_BYTES);
-    int32_t* ob_p = ob_b + OB;
-    TableSlot<K> table;
-    table.bind(reinterpret_cast<uint8_t*>(ob_p + OB), a.table_slots);
-    __shared__ uint64_t bars[NSTAGE];
-    __shared__ int64_t s_item;
-    __shared__ int s_obn;
-    __shared__ unsigned long long s_gpos;
+    uint8_t* table = smem;
+    uint32_t* ends = reinterpret_cast<uint32_t*>(smem + SM::entries_bytes(a.cap));
+    constexpr int STAGE = 32 * U;  // staged entries per warp
+    int32_t* stage_b = reinterpret_cast<int32_t*>(smem + SM::table_bytes(a.cap, a.nb_log2)) + warp_id() * 2 * STAGE;
+    int32_t* stage_p = stage_b + STAGE;
+    // OPEN tables of 8-byte keys: keys[cap] (8 B) then rows[cap]
+    unsigned long long* okeys = reinterpret_cast<unsigned long long*>(table);
+    uint32_t* orows = reinterpret_cast<uint32_t*>(table + static_cast<size_t>(a.cap) * 8);
 
-    const int T = a.table_slots;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
+    __shared__ int64_t s_item, s_next;
+    __shared__ uint32_t s_q;                  // entries this CTA produced
+    __shared__ long long s_cbase[OUT_SLOTS];  // output chunk bases
+    __shared__ int s_cid[OUT_SLOTS];          // chunk number held by each slot
+    __shared__ uint32_t s_warp[NWARPS];
+    __shared__ int s_nbuild;
 
-    BulkRing<NSTAGE, SM::STAGE_BYTES> ring;
-    ring.stages = stages;
-    ring.bars = bars;
-    ring.phase_bits = 0;
-    ring.init_barriers();
-    if (threadIdx.x == 0) s_obn = 0;
+    const int NB = 1 << a.nb_log2;
+    const uint32_t nb_mask = static_cast<uint32_t>(NB - 1);
     const int64_t total_items = a.item_off[a.P];
+    const bool write_out = a.out_build != nullptr;
 
-    auto flush = [&]() {
-        if (threadIdx.x == 0) s_gpos = atomicAdd(a.count, static_cast<unsigned long long>(s_obn));
-        __syncthreads();
-        const int n = s_obn;
-        const int64_t g = static_cast<int64_t>(s_gpos);
-        if (g + n > a.capacity && threadIdx.x == 0) raise_status(a.status, ST_CAPACITY);
-        for (int i = threadIdx.x; i < n; i += THREADS) {
-            if (g + i < a.capacity) {
-                a.out_build[g + i] = ob_b[i];
-                a.out_probe[g + i] = ob_p[i];
-            }
+    if (threadIdx.x == 0) {
+        s_q = 0;
+        s_next = static_cast<int64_t>(atomicAdd(a.queue, 1u));
+    }
+    if (threadIdx.x < OUT_SLOTS) s_cid[threadIdx.x] = -1;
+
+    // -- output ------------------------------------------------------------
+    // Base of output chunk ch: reserved with one global atomic by the lane
+    // whose entries include the chunk's first position, read by the others.
+    auto chunk_base = [&](uint32_t ch, bool reserve) -> long long {
+        const int slot = static_cast<int>(ch % OUT_SLOTS);
+        volatile int* vcid = s_cid;
+        volatile long long* vbase = s_cbase;
+        if (reserve) {
+            const long long g = static_cast<long long>(atomicAdd(a.count, static_cast<unsigned long long>(OUT_CHUNK)));
+            vbase[slot] = g;
+            __threadfence_block();
+            vcid[slot] = static_cast<int>(ch);
+            return g;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) s_obn = 0;
-        __syncthreads();
+        uint32_t spins = 0;
+        for (;;) {
+            const int c = vcid[slot];
+            if (c == static_cast<int>(ch)) break;
+            if (c > static_cast<int>(ch)) {  // slot reused: cannot happen with OUT_SLOTS of slack
+                raise_status(a.status, ST_INTERNAL);
+                return -1;
+            }
+            if (++spins > SPIN_LIMIT) {
+                raise_status(a.status, ST_TIMEOUT);
+                return -1;
+            }
+            __nanosleep(20);
+        }
+        __threadfence_block();
+        return vbase[slot];
+    };
+    auto store_out = [&](long long pos, int32_t b, int32_t q) {
+        if (pos < a.capacity) {
+            a.out_build[pos] = b;
+            a.out_probe[pos] = q;
+        } else if (pos - a.capacity < a.over_cap) {
+            a.over_build[pos - a.capacity] = b;
+            a.over_probe[pos - a.capacity] = q;
+        } else {
+            raise_status(a.status, ST_CAPACITY);
+        }
+    };
+    // Whole warp: every lane appends its c entries; put(stage_index) writes
+    // them into the warp's staging buffer.
+    auto append = [&](int c, auto&& put) {
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int n = __shfl_sync(0xffffffffu, incl, 31);
+        if (n == 0) return;
+        uint32_t q0 = 0;
+        if (lane == 0) q0 = atomicAdd(&s_q, static_cast<uint32_t>(n));
+        q0 = __shfl_sync(0xffffffffu, q0, 0);
+        if (!write_out) return;  // count only
+        put(incl - c);
+        __syncwarp();
+        const uint32_t ch0 = q0 / OUT_CHUNK, ch1 = (q0 + n - 1) / OUT_CHUNK;
+        long long b0 = 0, b1 = 0;
+        if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
+        if (lane == 1 && ch1 != ch0) b1 = chunk_base(ch1, true);  // its first position is ours
+        b0 = __shfl_sync(0xffffffffu, b0, 0);
+        b1 = __shfl_sync(0xffffffffu, b1, 1);
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t q = q0 + static_cast<uint32_t>(i);
+            const long long base = q / OUT_CHUNK == ch0 ? b0 : b1;
+            if (base >= 0) store_out(base + q % OUT_CHUNK, stage_b[i], stage_p[i]);
+        }
+        __syncwarp();
     };
 
     for (;;) {
-        if (threadIdx.x == 0) s_item = static_cast<int64_t>(atomicAdd(a.queue, 1u));
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_item = s_next;
+            s_next = static_cast<int64_t>(atomicAdd(a.queue, 1u));  // claim the next item early
+        }
         __syncthreads();
         const int64_t item = s_item;
-        if (item >= total_items) break;
-        const int p = upper_bound_i64(a.item_off, a.P + 1, item) - 1;
+        if (item >= total_items || item >= a.max_items) break;
+        // first link of the next item's metadata chain, used at the probe start
+        int next_p = -1;
+        if (threadIdx.x == 0 && s_next < total_items && s_next < a.max_items) next_p = a.item_part[s_next];
+        const int p = a.item_part[item];
         const int64_t local = item - a.item_off[p];
-        const int32_t split = a.split_log2[p];
+        const int32_t split = a.split[p];
         const int64_t S = HASH_SPLIT ? (1ll << split) : split;
         const int64_t piece = local % S;
         const int64_t pchunk = local / S;
         const int sbits = HASH_SPLIT ? split : 0;
         const int skip = a.digit_bits + sbits;
+        const int piece_shift = 32 - (sbits > 0 ? sbits : 1);
 
         const int64_t b_lo0 = a.build_off[static_cast<int64_t>(p) * a.b_items];
         const int64_t b_hi0 = a.build_off[static_cast<int64_t>(p + 1) * a.b_items];
         int64_t b_lo = b_lo0, b_hi = b_hi0;
         if (!HASH_SPLIT) {
-            // position pieces of position_chunk tuples, rounded to 16-byte multiples
             b_lo = b_lo0 + piece * a.position_chunk;
             b_hi = b_lo + a.position_chunk < b_hi0 ? b_lo + a.position_chunk : b_hi0;
             if (b_lo > b_hi) b_lo = b_hi;
@@ -260,117 +419,411 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         const int64_t q_lo = q_lo0 + pchunk * a.probe_chunk;
         const int64_t q_hi = q_lo + a.probe_chunk < q_hi0 ? q_lo + a.probe_chunk : q_hi0;
 
-        // the sbits hash bits just below the digit bits select the piece
-        const int piece_shift = 32 - (sbits > 0 ? sbits : 1);
+        // the probe chunk streams into L2 while the table is built
+        if (threadIdx.x == 0) prefetch_l2(a.probe_tuples + (q_lo * TV::WORDS), (q_hi - q_lo) * TV::WORDS * 4);
+
         auto in_piece = [&](uint32_t h) -> bool {
             if (!HASH_SPLIT || sbits == 0) return true;
             return static_cast<int64_t>((h << a.digit_bits) >> piece_shift) == piece;
         };
-        auto slot_of = [&](uint32_t h) -> int {
-            return SLOT_REF ? static_cast<int>(slot_ref(h, T)) : static_cast<int>(slot_fast(h, skip, T));
+        auto bucket_of = [&](uint32_t h) -> uint32_t { return h & nb_mask; };
+        auto slot_of = [&](uint32_t h) -> uint32_t {
+            return SLOT_REF ? slot_ref(h, a.cap) : slot_fast(h, skip, static_cast<uint32_t>(a.cap));
         };
 
-        for (int i = threadIdx.x; i < T; i += THREADS) table.clear(i);
-        __syncthreads();
-
         // ---- build ----
-        ring.start(a.build_tuples + (b_lo * SM::TB) / 4, (b_hi - b_lo) * SM::TB, a.status);
-        {
-            const int64_t nch = ring.num_chunks();
-            for (int64_t c = 0; c < nch; ++c) {
-                const uint8_t* st = ring.wait(c);
-                const int64_t left = (b_hi - b_lo) - c * STAGE_TUPLES;
-                const int cnt = left < STAGE_TUPLES ? static_cast<int>(left) : STAGE_TUPLES;
-                for (int j = threadIdx.x; j < cnt; j += THREADS) {
-                    K key;
-                    int32_t row;
-                    smem_tuple<K>(st, j, key, row);
-                    if (row < 0) continue;
-                    const uint32_t h = hash_key(key);
-                    if (!in_piece(h)) continue;
-                    int sl = slot_of(h);
-                    int tries = 0;
-                    while (!table.try_claim(sl, key, row)) {
-                        if (++sl == T) sl = 0;
-                        if (++tries >= T) {
-                            raise_status(a.status, ST_OVERFLOW);
-                            break;
+        bool skip_item = false;
+        if constexpr (TABLE == TABLE_BUCKET) {
+            for (int i = threadIdx.x; i < NB / 2; i += THREADS) ends[i] = 0u;
+            if (threadIdx.x == 0) s_nbuild = 0;
+            __syncthreads();
+            // pass 1: count per bucket; the next batch of loads is issued
+            // before the current one is counted
+            int mine = 0;
+            {
+                uint32_t nh[JOIN_BU];
+                Cmp nk[JOIN_BU];
+                int32_t nr[JOIN_BU];
+                auto load_batch = [&](int64_t i0) {
+#pragma unroll
+                    for (int u = 0; u < JOIN_BU; ++u) {
+                        const int64_t i = i0 + u * THREADS;
+                        nr[u] = -1;
+                        if (i < b_hi) TV::load(a.build_tuples, i, nh[u], nk[u], nr[u]);
+                    }
+                };
+                int64_t i0 = b_lo + threadIdx.x;
+                if (i0 < b_hi) load_batch(i0);
+                for (; i0 < b_hi; i0 += THREADS * JOIN_BU) {
+                    uint32_t h[JOIN_BU];
+                    int32_t r[JOIN_BU];
+#pragma unroll
+                    for (int u = 0; u < JOIN_BU; ++u) {
+                        h[u] = nh[u];
+                        r[u] = nr[u];
+                    }
+                    if (i0 + THREADS * JOIN_BU < b_hi) load_batch(i0 + THREADS * JOIN_BU);
+#pragma unroll
+                    for (int u = 0; u < JOIN_BU; ++u) {
+                        if (r[u] >= 0 && in_piece(h[u])) {
+                            const uint32_t b = bucket_of(h[u]);
+                            atomicAdd(&ends[b >> 1], (b & 1u) ? 0x10000u : 1u);
+                            ++mine;
                         }
                     }
                 }
-                __syncthreads();
-                ring.release(c);
             }
-        }
-        __syncthreads();
-
-        // ---- probe ----
-        ring.start(a.probe_tuples + (q_lo * SM::TB) / 4, (q_hi - q_lo) * SM::TB, a.status);
-        {
-            const int64_t nch = ring.num_chunks();
-            for (int64_t c = 0; c < nch; ++c) {
-                const uint8_t* st = ring.wait(c);
-                const int64_t left = (q_hi - q_lo) - c * STAGE_TUPLES;
-                const int cnt = left < STAGE_TUPLES ? static_cast<int>(left) : STAGE_TUPLES;
-                const int64_t row_base = 0;
-                (void)row_base;
-                for (int r0 = 0; r0 < cnt; r0 += THREADS) {
-                    const int j = r0 + threadIdx.x;
-                    K key = K(0);
-                    int32_t prow = -1;
-                    bool pending = false;
-                    int sl = 0, steps = 0;
-                    if (j < cnt) {
-                        smem_tuple<K>(st, j, key, prow);
-                        if (prow >= 0) {
-                            const uint32_t h = hash_key(key);
-                            if (in_piece(h)) {
-                                pending = true;
-                                sl = slot_of(h);
-                            }
+            mine = __reduce_add_sync(0xffffffffu, mine);
+            if (lane == 0 && mine) atomicAdd(&s_nbuild, mine);
+            __syncthreads();
+            if (s_nbuild > a.cap) {  // the planner sizes pieces to fit; flag and skip
+                if (threadIdx.x == 0) raise_status(a.status, ST_OVERFLOW);
+                skip_item = true;
+            } else {
+                scan_u16_pairs<THREADS>(ends, NB / 2, s_warp);
+                // pass 2: place
+                for (int64_t i0 = b_lo + threadIdx.x; i0 < b_hi; i0 += THREADS * JOIN_BU) {
+                    uint32_t h[JOIN_BU];
+                    Cmp k[JOIN_BU];
+                    int32_t r[JOIN_BU];
+#pragma unroll
+                    for (int u = 0; u < JOIN_BU; ++u) {
+                        const int64_t i = i0 + u * THREADS;
+                        r[u] = -1;
+                        if (i < b_hi) TV::load(a.build_tuples, i, h[u], k[u], r[u]);
+                    }
+#pragma unroll
+                    for (int u = 0; u < JOIN_BU; ++u) {
+                        if (r[u] >= 0 && in_piece(h[u])) {
+                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t old = atomicAdd(&ends[b >> 1], (b & 1u) ? 0x10000u : 1u);
+                            const int pos = static_cast<int>((b & 1u) ? (old >> 16) : (old & 0xffffu));
+                            E::put(table, pos, k[u], r[u]);
                         }
                     }
-                    bool more;
-                    do {
-                        // walk to the next match (or an empty slot)
-                        bool emit = false;
-                        uint32_t brow = 0;
-                        while (pending) {
-                            bool hit;
-                            const uint32_t rw = table.look(sl, key, hit);
-                            if (rw == EMPTY_ROW) { pending = false; break; }
-                            if (++sl == T) sl = 0;
-                            if (++steps > T) { pending = false; break; }
-                            if (hit) {
-                                emit = true;
-                                brow = rw;
-                                if (UNIQUE) pending = false;
+                }
+            }
+            __syncthreads();
+        } else {
+            for (int i = threadIdx.x; i < a.cap; i += THREADS) {
+                if constexpr (sizeof(K) == 4) reinterpret_cast<uint2*>(table)[i] = make_uint2(0u, EMPTY_ROW);
+                else orows[i] = EMPTY_ROW;
+            }
+            __syncthreads();
+            for (int64_t i = b_lo + threadIdx.x; i < b_hi; i += THREADS) {
+                uint32_t h;
+                Cmp k;
+                int32_t r;
+                TV::load(a.build_tuples, i, h, k, r);
+                if (r < 0 || !in_piece(h)) continue;
+                uint32_t sl = slot_of(h);
+                int tries = 0;
+                for (;;) {
+                    uint32_t* rw = sizeof(K) == 4 ? &reinterpret_cast<uint2*>(table)[sl].y : &orows[sl];
+                    if (atomicCAS(rw, EMPTY_ROW, static_cast<uint32_t>(r)) == EMPTY_ROW) {
+                        if constexpr (sizeof(K) == 4) reinterpret_cast<uint2*>(table)[sl].x = static_cast<uint32_t>(k);
+                        else okeys[sl] = k;
+                        break;
+                    }
+                    if (++sl == static_cast<uint32_t>(a.cap)) sl = 0;
+                    if (++tries >= a.cap) {
+                        raise_status(a.status, ST_OVERFLOW);
+                        break;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+
+        // the next item's build side streams into L2 while this item probes
+        if (threadIdx.x == 0 && next_p >= 0 && next_p != p) {
+            const int64_t nb_lo = a.build_off[static_cast<int64_t>(next_p) * a.b_items];
+            const int64_t nb_hi = a.build_off[static_cast<int64_t>(next_p + 1) * a.b_items];
+            const int64_t nbytes = (nb_hi - nb_lo) * TV::WORDS * 4;
+            prefetch_l2(a.build_tuples + nb_lo * TV::WORDS, nbytes < (1 << 20) ? nbytes : (1 << 20));
+        }
+
+        // ---- probe: warps run independently; loads run one step ahead ----
+        if (!skip_item) {
+            const int64_t per_step = static_cast<int64_t>(NWARPS) * 32 * U;
+            uint32_t nh[U];
+            Cmp nk[U];
+            int32_t nr[U];
+            auto load_step = [&](int64_t s0) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t i = s0 + u * 32 + lane;
+                    nr[u] = -1;
+                    if (i < q_hi) TV::load(a.probe_tuples, i, nh[u], nk[u], nr[u]);
+                }
+            };
+            int64_t s0 = q_lo + static_cast<int64_t>(warp) * 32 * U;
+            if (s0 < q_hi) load_step(s0);
+            for (; s0 < q_hi; s0 += per_step) {
+                uint32_t h[U];
+                Cmp k[U];
+                int32_t r[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    h[u] = nh[u];
+                    k[u] = nk[u];
+                    r[u] = nr[u];
+                }
+                if (s0 + per_step < q_hi) load_step(s0 + per_step);
+                // look up one tuple from (at, end) or slot sl; returns whether a match was found
+                auto lookup = [&](int u, int& at_u, int end_u, uint32_t& sl_u, int& steps_u, bool& live_u,
+                                  uint32_t& brow_u) -> bool {
+                    bool found = false;
+                    if constexpr (TABLE == TABLE_BUCKET) {
+                        while (at_u < end_u) {
+                            Cmp ek;
+                            uint32_t er;
+                            E::get(table, at_u, ek, er);
+                            ++at_u;
+                            if (ek == k[u]) {
+                                found = true;
+                                brow_u = er;
                                 break;
                             }
                         }
-                        const unsigned m = __ballot_sync(0xffffffffu, emit);
-                        if (m) {
-                            const int leader = __ffs(m) - 1;
-                            int base = 0;
-                            if (lane == leader) base = atomicAdd(&s_obn, __popc(m));
-                            base = __shfl_sync(0xffffffffu, base, leader);
-                            if (emit) {
-                                const int at = base + __popc(m & lt_mask);
-                                ob_b[at] = static_cast<int32_t>(brow);
-                                ob_p[at] = prow;
+                        if (!found || UNIQUE) live_u = false;
+                    } else {
+                        for (;;) {
+                            Cmp ek;
+                            uint32_t er;
+                            if constexpr (sizeof(K) == 4) {
+                                const uint2 v = reinterpret_cast<const uint2*>(table)[sl_u];
+                                ek = v.x;
+                                er = v.y;
+                            } else {
+                                er = orows[sl_u];
+                                ek = okeys[sl_u];
+                            }
+                            if (er == EMPTY_ROW) { live_u = false; break; }
+                            if (++sl_u == static_cast<uint32_t>(a.cap)) sl_u = 0;
+                            if (++steps_u > a.cap) { live_u = false; break; }
+                            if (ek == k[u]) {
+                                found = true;
+                                brow_u = er;
+                                if (UNIQUE) live_u = false;
+                                break;
                             }
                         }
-                        more = __syncthreads_or(pending) != 0;
-                        if (s_obn > OB - THREADS) flush();
-                    } while (more);
+                    }
+                    return found;
+                };
+                auto start = [&](int u, int& at_u, int& end_u, uint32_t& sl_u) {
+                    if constexpr (TABLE == TABLE_BUCKET) {
+                        const uint32_t b = bucket_of(h[u]);
+                        end_u = static_cast<int>((ends[b >> 1] >> ((b & 1u) * 16)) & 0xffffu);
+                        at_u = b == 0 ? 0 : static_cast<int>((ends[(b - 1) >> 1] >> (((b - 1) & 1u) * 16)) & 0xffffu);
+                    } else {
+                        sl_u = slot_of(h[u]);
+                    }
+                };
+                if constexpr (UNIQUE) {
+                    // every tuple matches at most once: one lookup, one append per warp step
+                    bool emit[U];
+                    uint32_t brow[U];
+                    int c = 0;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        emit[u] = false;
+                        brow[u] = 0;
+                        if (r[u] >= 0 && in_piece(h[u])) {
+                            int at_u = 0, end_u = 0, steps_u = 0;
+                            uint32_t sl_u = 0;
+                            bool live_u = true;
+                            start(u, at_u, end_u, sl_u);
+                            emit[u] = lookup(u, at_u, end_u, sl_u, steps_u, live_u, brow[u]);
+                        }
+                        c += emit[u] ? 1 : 0;
+                    }
+                    append(c, [&](int at_stage) {
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+                            if (emit[u]) {
+                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
+                                stage_p[at_stage] = r[u];
+                                ++at_stage;
+                            }
+                    });
+                } else {
+                    // repeated build keys: every tuple walks on, one match per lane per append
+                    bool live[U], emit[U];
+                    uint32_t brow[U], sl[U];
+                    int at[U], end[U], steps[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        live[u] = r[u] >= 0 && in_piece(h[u]);
+                        at[u] = end[u] = steps[u] = 0;
+                        sl[u] = 0;
+                        brow[u] = 0;
+                        if (live[u]) start(u, at[u], end[u], sl[u]);
+                    }
+                    for (;;) {
+                        int c = 0;
+                        bool any_live = false;
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            emit[u] = live[u] && lookup(u, at[u], end[u], sl[u], steps[u], live[u], brow[u]);
+                            c += emit[u] ? 1 : 0;
+                            any_live |= live[u];
+                        }
+                        append(c, [&](int at_stage) {
+#pragma unroll
+                            for (int u = 0; u < U; ++u)
+                                if (emit[u]) {
+                                    stage_b[at_stage] = static_cast<int32_t>(brow[u]);
+                                    stage_p[at_stage] = r[u];
+                                    ++at_stage;
+                                }
+                        });
+                        if (!__any_sync(0xffffffffu, any_live)) break;
+                    }
                 }
-                __syncthreads();
-                ring.release(c);
             }
         }
-        __syncthreads();
     }
-    if (s_obn > 0) flush();
+    // ---- record this CTA's entries and last chunk for the fix-up ----
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t q = s_q;
+        a.cta_q[blockIdx.x] = q;
+        a.cta_last[blockIdx.x] = (q > 0 && write_out) ? s_cbase[((q - 1) / OUT_CHUNK) % OUT_SLOTS] : -1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fix-up of the output.  The CTAs' reservations cover [0, reserved); CTA c
+// used the first cta_q[c] % OUT_CHUNK entries of its last chunk, so the
+// rest of that chunk is a gap.  total = sum cta_q.  Every gap position below
+// total is filled with a valid entry from at or above total (those lie in
+// [total, reserved) outside the gaps), in order: no two moves touch the
+// same position and sources never overlap destinations.
+// Plan (one CTA): sorted gaps -> hole segments (< total) and mover
+// segments (>= total), their prefix sums; *count = total.
+// seg layout: [0] = n_holes, [1] = n_movers, [2] = moves; then
+// hole (start, prefix) pairs, then mover (start, prefix) pairs.
+__global__ void __launch_bounds__(1024) join_fixup_plan_kernel(const int64_t* __restrict__ cta_q,
+                                                               const int64_t* __restrict__ cta_last, int32_t n_cta,
+                                                               unsigned long long* count, int64_t capacity,
+                                                               int32_t write_out, int64_t* __restrict__ seg,
+                                                               uint32_t* __restrict__ status)
+{
+    __shared__ long long s_sum;
+    __shared__ long long g_start[1024], g_len[1024];
+    __shared__ int s_ng;
+    if (threadIdx.x == 0) {
+        s_sum = 0;
+        s_ng = 0;
+    }
+    __syncthreads();
+    long long mine = 0;
+    for (int c = threadIdx.x; c < n_cta; c += blockDim.x) mine += cta_q[c];
+    atomicAdd(reinterpret_cast<unsigned long long*>(&s_sum), static_cast<unsigned long long>(mine));
+    // gaps, placed at their rank by start (starts are distinct chunk positions)
+    long long my_start = -1, my_len = 0;
+    if (threadIdx.x < n_cta && write_out) {
+        const long long q = cta_q[threadIdx.x], rem = q % OUT_CHUNK;
+        if (q > 0 && rem != 0 && cta_last[threadIdx.x] >= 0) {
+            my_start = cta_last[threadIdx.x] + rem;
+            my_len = OUT_CHUNK - rem;
+        }
+    }
+    __syncthreads();
+    if (my_start >= 0) {
+        int rank = 0;
+        for (int c = 0; c < n_cta; ++c) {
+            const long long q = cta_q[c], rem = q % OUT_CHUNK;
+            if (q > 0 && rem != 0 && cta_last[c] >= 0 && cta_last[c] + rem < my_start) ++rank;
+        }
+        g_start[rank] = my_start;
+        g_len[rank] = my_len;
+        atomicAdd(&s_ng, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long total = s_sum;
+        const long long reserved = static_cast<long long>(*count);
+        *count = static_cast<unsigned long long>(total);
+        int nh = 0, nm = 0;
+        long long moves = 0;
+        if (write_out && total <= capacity) {
+            int64_t* hole = seg + 4;
+            int64_t* mover = seg + 4 + 2 * (n_cta + 2);
+            long long hp = 0, mp = 0, cur = total;
+            for (int g = 0; g < s_ng; ++g) {
+                const long long gs = g_start[g], ge = g_start[g] + g_len[g];
+                if (gs < total) {  // hole: the part of the gap below total
+                    hole[2 * nh] = gs;
+                    hole[2 * nh + 1] = hp;
+                    hp += (ge < total ? ge : total) - gs;
+                    ++nh;
+                }
+                if (ge <= cur) continue;
+                if (gs > cur) {  // valid entries between the previous gap and this one
+                    const long long e = gs < reserved ? gs : reserved;
+                    if (e > cur) {
+                        mover[2 * nm] = cur;
+                        mover[2 * nm + 1] = mp;
+                        mp += e - cur;
+                        ++nm;
+                    }
+                }
+                if (ge > cur) cur = ge;
+            }
+            if (cur < reserved) {
+                mover[2 * nm] = cur;
+                mover[2 * nm + 1] = mp;
+                mp += reserved - cur;
+                ++nm;
+            }
+            if (hp != mp) raise_status(status, ST_INTERNAL);
+            moves = hp < mp ? hp : mp;
+        } else if (write_out && total > capacity) {
+            raise_status(status, ST_CAPACITY);
+        }
+        seg[0] = nh;
+        seg[1] = nm;
+        seg[2] = moves;
+    }
+}
+
+__device__ __forceinline__ int seg_find(const int64_t* s, int n, long long i)
+{
+    int lo = 0, hi = n;  // last segment with prefix <= i
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s[2 * mid + 1] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void join_fixup_move_kernel(const int64_t* __restrict__ seg, int32_t n_cta, int32_t* out_build,
+                                       int32_t* out_probe, int64_t capacity, const int32_t* __restrict__ over_build,
+                                       const int32_t* __restrict__ over_probe)
+{
+    const int nh = static_cast<int>(seg[0]), nm = static_cast<int>(seg[1]);
+    const long long moves = seg[2];
+    const int64_t* hole = seg + 4;
+    const int64_t* mover = seg + 4 + 2 * (n_cta + 2);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < moves;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int h = seg_find(hole, nh, i), m = seg_find(mover, nm, i);
+        const long long dst = hole[2 * h] + (i - hole[2 * h + 1]);
+        const long long src = mover[2 * m] + (i - mover[2 * m + 1]);
+        int32_t b, q;
+        if (src < capacity) {
+            b = out_build[src];
+            q = out_probe[src];
+        } else {
+            b = over_build[src - capacity];
+            q = over_probe[src - capacity];
+        }
+        out_build[dst] = b;
+        out_probe[dst] = q;
+    }
 }
 
 }  // namespace pj

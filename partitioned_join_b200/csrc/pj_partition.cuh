@@ -7,29 +7,29 @@
 // of the output, where off is the exclusive scan of the per-(p, i) counts,
 // each rounded up to W tuples.  So partitions are contiguous
 // (partition p = [off[p*n_items], off[(p+1)*n_items]) ), every segment starts
-// on a W-tuple boundary (one or more whole 32-byte sectors), and the padding
-// tuples that fill a segment's last W-group carry row = -1.
+// on a W-tuple boundary, and the padding tuples that fill a segment's last
+// W-group carry row = -1.
+//
+// Tuples.  4-byte keys are stored as {murmur(key), row}: MurmurHash3_x86_32
+// of a 4-byte key is a bijection of 32-bit values (every step -- odd
+// multiplies, rotations, xor/add of constants, the fmix32 xor-shifts -- is
+// invertible), so equal hashes mean equal keys and the join never hashes
+// again.  8-byte keys are stored as {key_lo, key_hi, row}.
 //
 // Reference counterparts: histogram_pass_one (partition_kernels.cuh:141-194),
 // the ExclusiveSum + copy of partitioned_join.cuh:86-88, partition_pass_one
 // (partition_kernels.cuh:197-326).  The reference stages an 8 192-key tile in
 // shared memory and flushes each partition's run with 32 threads; here each
-// CTA keeps a W-tuple write-combining buffer per partition and only ever
-// writes whole aligned sectors, so the DRAM sees full-sector writes at any
-// fan-out.
+// CTA keeps a W-tuple write-combining buffer per partition and writes only
+// whole, aligned W-tuple groups, so the fan-out of one pass can be 8 192.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "pj_bulk.cuh"
 #include "pj_device.cuh"
 
 namespace pj {
-
-constexpr int HIST_THREADS = 1024;
-constexpr int HIST_V = 4;       // keys per thread per round
-constexpr int HIST_NSTAGE = 3;
 
 template <typename K>
 __device__ __forceinline__ uint32_t key_digit(const DigitFn& f, K key)
@@ -37,64 +37,79 @@ __device__ __forceinline__ uint32_t key_digit(const DigitFn& f, K key)
     return digit_of(f, key, f.mode == 1 ? hash_key(key) : 0u);
 }
 
-// Per-(partition, item) histogram of one key column.  counts_T[p*n_items+i]
-// (p-major, the order the scan wants) and, if totals != nullptr,
-// atomicAdd of every partition's count into totals[p].
+// Elements of a 16-byte vector.
+template <typename K> struct Vec16 { static constexpr int N = 16 / sizeof(K); };
+
 template <typename K>
-__global__ void __launch_bounds__(HIST_THREADS) hist_keys_kernel(const K* __restrict__ keys, int64_t n,
-                                                                 int64_t chunk, int32_t n_items, DigitFn f,
-                                                                 int32_t P, uint32_t* __restrict__ counts_T,
-                                                                 int32_t* __restrict__ totals,
-                                                                 uint32_t* __restrict__ status)
+__device__ __forceinline__ void load_vec16(const K* p, K (&out)[Vec16<K>::N])
 {
-    constexpr int ROUND = HIST_THREADS * HIST_V;
-    constexpr int STAGE_BYTES = ROUND * static_cast<int>(sizeof(K));
-    extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* stages = smem;
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(smem + HIST_NSTAGE * STAGE_BYTES);
-    __shared__ uint64_t bars[HIST_NSTAGE];
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+    if constexpr (sizeof(K) == 4) {
+        out[0] = static_cast<K>(v.x); out[1] = static_cast<K>(v.y);
+        out[2] = static_cast<K>(v.z); out[3] = static_cast<K>(v.w);
+    } else {
+        out[0] = static_cast<K>((static_cast<uint64_t>(v.y) << 32) | v.x);
+        out[1] = static_cast<K>((static_cast<uint64_t>(v.w) << 32) | v.z);
+    }
+}
 
-    BulkRing<HIST_NSTAGE, STAGE_BYTES> ring;
-    ring.stages = stages;
-    ring.bars = bars;
-    ring.phase_bits = 0;
-    ring.init_barriers();
+// ---------------------------------------------------------------------------
+// Histogram.  Grid = n_items * hsplit CTAs; CTA c counts the keys of the
+// (c % hsplit)-th slice of item c / hsplit's chunk in shared memory and adds
+// them into counts_T[p*n_items + item] (zeroed by the caller) and totals[p].
+constexpr int HIST_THREADS = 512;
+constexpr int HIST_UNROLL = 4;  // 16-byte vectors in flight per thread
 
-    for (int32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-        for (int p = threadIdx.x; p < P; p += HIST_THREADS) cnt[p] = 0;
-        __syncthreads();
-        int64_t lo = static_cast<int64_t>(item) * chunk;
-        int64_t hi = lo + chunk < n ? lo + chunk : n;
-        if (lo > hi) lo = hi;
-        const int64_t bulk_keys = (((hi - lo) * static_cast<int64_t>(sizeof(K))) & ~int64_t(15)) / sizeof(K);
-        ring.start(keys + lo, bulk_keys * static_cast<int64_t>(sizeof(K)), status);
-        const int64_t nch = ring.num_chunks();
-        for (int64_t c = 0; c < nch; ++c) {
-            const K* sk = reinterpret_cast<const K*>(ring.wait(c));
-            const int64_t left = bulk_keys - c * ROUND;
-            const int cntk = left < ROUND ? static_cast<int>(left) : ROUND;
+template <typename K, bool HASHD>
+__global__ void __launch_bounds__(HIST_THREADS) hist_keys_kernel(const K* __restrict__ keys, int64_t n,
+                                                                 int64_t chunk, int32_t n_items, int32_t hsplit,
+                                                                 DigitFn f, int32_t P,
+                                                                 uint32_t* __restrict__ counts_T,
+                                                                 int32_t* __restrict__ totals)
+{
+    constexpr int VN = Vec16<K>::N;
+    extern __shared__ __align__(16) uint32_t cnt[];
+    const int item = blockIdx.x / hsplit, part = blockIdx.x % hsplit;
+    for (int p = threadIdx.x; p < P; p += HIST_THREADS) cnt[p] = 0;
+    __syncthreads();
+    int64_t lo = static_cast<int64_t>(item) * chunk;
+    int64_t hi = lo + chunk < n ? lo + chunk : n;
+    if (lo > hi) lo = hi;
+    // this CTA's slice of the item, 16-element aligned
+    const int64_t per = (((hi - lo) + hsplit - 1) / hsplit + 15) & ~int64_t(15);
+    int64_t s_lo = lo + part * per;
+    int64_t s_hi = s_lo + per < hi ? s_lo + per : hi;
+    if (s_lo > s_hi) s_lo = s_hi;
+    auto count = [&](K k) {
+        const uint32_t d = HASHD ? ((hash_key(k) >> f.shift) & f.mask)
+                                 : (static_cast<uint32_t>(static_cast<uint64_t>(k) >> f.shift) & f.mask);
+        atomicAdd(&cnt[d], 1u);
+    };
+    constexpr int STEP = HIST_THREADS * VN * HIST_UNROLL;
+    int64_t base = s_lo;
+    for (; base + STEP <= s_hi; base += STEP) {
+        K v[HIST_UNROLL][VN];
 #pragma unroll
-            for (int v = 0; v < HIST_V; ++v) {
-                const int j = v * HIST_THREADS + threadIdx.x;
-                if (j < cntk) atomicAdd(&cnt[key_digit(f, sk[j])], 1u);
-            }
-            __syncthreads();
-            ring.release(c);
+        for (int u = 0; u < HIST_UNROLL; ++u)
+            load_vec16<K>(keys + base + (static_cast<int64_t>(u) * HIST_THREADS + threadIdx.x) * VN, v[u]);
+#pragma unroll
+        for (int u = 0; u < HIST_UNROLL; ++u)
+#pragma unroll
+            for (int e = 0; e < VN; ++e) count(v[u][e]);
+    }
+    for (int64_t i = base + threadIdx.x; i < s_hi; i += HIST_THREADS) count(keys[i]);
+    __syncthreads();
+    for (int p = threadIdx.x; p < P; p += HIST_THREADS) {
+        const uint32_t c = cnt[p];
+        if (c) {
+            atomicAdd(&counts_T[static_cast<int64_t>(p) * n_items + item], c);
+            if (totals != nullptr) atomicAdd(&totals[p], static_cast<int32_t>(c));
         }
-        for (int64_t j = lo + bulk_keys + threadIdx.x; j < hi; j += HIST_THREADS)
-            atomicAdd(&cnt[key_digit(f, keys[j])], 1u);
-        __syncthreads();
-        for (int p = threadIdx.x; p < P; p += HIST_THREADS) {
-            const uint32_t c = cnt[p];
-            counts_T[static_cast<int64_t>(p) * n_items + item] = c;
-            if (totals != nullptr && c) atomicAdd(&totals[p], static_cast<int32_t>(c));
-        }
-        __syncthreads();
     }
 }
 
 // Global digit histogram (no per-item split): the stage entry point
-// pj_radix_histogram and the exact planner.  Grid-stride over the keys.
+// pj_radix_histogram and the exact planner.
 template <typename K>
 __global__ void __launch_bounds__(512) global_hist_kernel(const K* __restrict__ keys, int64_t n, DigitFn f,
                                                           int32_t P, int32_t* __restrict__ hist)
@@ -163,7 +178,6 @@ __global__ void __launch_bounds__(SCAN_THREADS) lookback_scan_kernel(const TIn* 
         v[j] = x;
         sum += x;
     }
-    // block exclusive scan of the per-thread sums
     int64_t incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -183,7 +197,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) lookback_scan_kernel(const TIn* 
     }
     __syncthreads();
     const int64_t block_total = s_warp[SCAN_THREADS / 32 - 1];
-    int64_t thread_excl = incl - sum + (warp > 0 ? s_warp[warp - 1] : 0);
+    const int64_t thread_excl = incl - sum + (warp > 0 ? s_warp[warp - 1] : 0);
 
     if (threadIdx.x == 0) {
         int64_t excl = 0;
@@ -229,195 +243,228 @@ __global__ void __launch_bounds__(SCAN_THREADS) lookback_scan_kernel(const TIn* 
 // Each round every thread holds V tuples.  Phase A: a shared atomicAdd on
 // the partition's fill counter gives each tuple its position s in the
 // partition's stream; s < W goes into the W-slot buffer.  Phase B: the tuple
-// that took position W-1 flushes the full buffer as whole sectors; tuples
-// with W <= s < Q (Q = fill rounded down to W, i.e. sectors completed
-// entirely inside this round) are stored straight to global memory.  Phase C:
-// the remaining tuples (s >= Q) refill the emptied buffer; the flusher moves
-// the partition cursor by Q.  Every tuple is placed in the round it is read,
-// whatever the skew.
+// that took position W-1 flushes the full buffer as one aligned group;
+// tuples with W <= s < Q (Q = fill rounded down to W: groups completed
+// entirely inside this round) are stored straight to global memory.
+// Phase C: the remaining tuples (s >= Q) refill the emptied buffer and the
+// flusher moves the partition cursor by Q.  Every tuple is placed in the
+// round it is read, whatever the skew.
 template <typename K, int W>
 struct WcTraits {
     static constexpr int TW = TupleTraits<K>::WORDS;
     static constexpr int BW = W * TW;  // words per buffer
-    static_assert((BW * 4) % 32 == 0, "a buffer must be whole 32-byte sectors");
+    static_assert((BW * 4) % 16 == 0, "a buffer must be whole 16-byte vectors");
 };
 
-template <typename K, int W, int V>
-__device__ __forceinline__ void wc_phase_a(const K (&key)[V], const int32_t (&row)[V], const bool (&ok)[V],
-                                           const uint32_t (&d)[V], int (&s)[V], uint32_t* buf, int* fill)
+template <typename K>
+__device__ __forceinline__ void tuple_words(uint32_t (&w)[TupleTraits<K>::WORDS], K key, int32_t row);
+
+template <>
+__device__ __forceinline__ void tuple_words<int32_t>(uint32_t (&w)[2], int32_t key, int32_t row)
 {
-    constexpr int TW = WcTraits<K, W>::TW, BW = WcTraits<K, W>::BW;
+    w[0] = hash_key(key);  // stored hash: the join compares and places by it
+    w[1] = static_cast<uint32_t>(row);
+}
+
+template <>
+__device__ __forceinline__ void tuple_words<int64_t>(uint32_t (&w)[3], int64_t key, int32_t row)
+{
+    const uint64_t u = static_cast<uint64_t>(key);
+    w[0] = static_cast<uint32_t>(u);
+    w[1] = static_cast<uint32_t>(u >> 32);
+    w[2] = static_cast<uint32_t>(row);
+}
+
+template <int TW>
+__device__ __forceinline__ void store_words(uint32_t* dst, const uint32_t (&w)[TW])
+{
+    if constexpr (TW == 2) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
+    } else {
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-        if (ok[v]) {
-            s[v] = atomicAdd(&fill[d[v]], 1);
-            if (s[v] < W) put_tuple_words<K>(buf + static_cast<size_t>(d[v]) * BW + s[v] * TW, key[v], row[v]);
-        }
+        for (int i = 0; i < TW; ++i) dst[i] = w[i];
     }
+}
+
+// One 32-byte store per sector: sm_100's 256-bit st.global makes every
+// flushed sector a single L2 write request (two 16-byte stores of one
+// sector are two requests, which bounds the scatter at the L2 request rate).
+__device__ __forceinline__ void st_global_v8(uint32_t* g, const uint4& a, const uint4& b)
+{
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(g), "r"(a.x), "r"(a.y), "r"(a.z),
+                 "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                 : "memory");
 }
 
 template <typename K, int W>
 __device__ __forceinline__ void wc_flush(const uint32_t* sbuf, uint32_t* gdst)
 {
     constexpr int BW = WcTraits<K, W>::BW;
+    if constexpr ((BW * 4) % 32 == 0) {
 #pragma unroll
-    for (int q = 0; q < BW / 4; ++q)
-        reinterpret_cast<uint4*>(gdst)[q] = reinterpret_cast<const uint4*>(sbuf)[q];
-}
-
-template <typename K, int W, int V>
-__device__ __forceinline__ void wc_phase_b(const K (&key)[V], const int32_t (&row)[V], const bool (&ok)[V],
-                                           const uint32_t (&d)[V], const int (&s)[V], int (&F)[V], int (&Q)[V],
-                                           const uint32_t* buf, const int* fill, const uint32_t* cursor,
-                                           uint32_t* __restrict__ out, uint32_t out_cap, uint32_t* status)
-{
-    constexpr int TW = WcTraits<K, W>::TW, BW = WcTraits<K, W>::BW;
+        for (int q = 0; q < BW / 8; ++q)
+            st_global_v8(gdst + 8 * q, reinterpret_cast<const uint4*>(sbuf)[2 * q],
+                         reinterpret_cast<const uint4*>(sbuf)[2 * q + 1]);
+    } else {
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-        if (ok[v]) {
-            F[v] = fill[d[v]];
-            Q[v] = F[v] - F[v] % W;
-            const uint32_t cur = cursor[d[v]];
-            if (s[v] == W - 1) {
-                if (cur + static_cast<uint32_t>(W) <= out_cap)
-                    wc_flush<K, W>(buf + static_cast<size_t>(d[v]) * BW, out + static_cast<size_t>(cur) * TW);
-                else
-                    raise_status(status, ST_INTERNAL);
-            } else if (s[v] >= W && s[v] < Q[v]) {
-                const uint32_t pos = cur + static_cast<uint32_t>(s[v]);
-                if (pos < out_cap)
-                    put_tuple_words<K>(out + static_cast<size_t>(pos) * TW, key[v], row[v]);
-                else
-                    raise_status(status, ST_INTERNAL);
-            }
-        }
+        for (int q = 0; q < BW / 4; ++q)
+            reinterpret_cast<uint4*>(gdst)[q] = reinterpret_cast<const uint4*>(sbuf)[q];
     }
 }
 
-template <typename K, int W, int V>
-__device__ __forceinline__ void wc_phase_c(const K (&key)[V], const int32_t (&row)[V], const bool (&ok)[V],
-                                           const uint32_t (&d)[V], const int (&s)[V], const int (&F)[V],
-                                           const int (&Q)[V], uint32_t* buf, int* fill, uint32_t* cursor)
-{
-    constexpr int TW = WcTraits<K, W>::TW, BW = WcTraits<K, W>::BW;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-        if (ok[v]) {
-            if (s[v] >= W && s[v] >= Q[v])
-                put_tuple_words<K>(buf + static_cast<size_t>(d[v]) * BW + (s[v] - Q[v]) * TW, key[v], row[v]);
-            if (s[v] == W - 1) {
-                cursor[d[v]] += static_cast<uint32_t>(Q[v]);
-                fill[d[v]] = F[v] - Q[v];
-            }
-        }
-    }
-}
-
-template <typename K>
-__device__ __forceinline__ void pad_tuple_words(uint32_t* dst)
-{
-    put_tuple_words<K>(dst, K(0), PAD_ROW);
-}
-
-// Shared memory of the scatter kernel: stages + buffers + fill + cursor.
-template <typename K, int THREADS, int V, int W, int NSTAGE>
+template <typename K, int THREADS, int V, int W>
 struct ScatterSmem {
-    static constexpr int ROUND = THREADS * V;
-    static constexpr int STAGE_BYTES = ROUND * static_cast<int>(sizeof(K));
     static size_t bytes(int P)
     {
-        return static_cast<size_t>(NSTAGE) * STAGE_BYTES + static_cast<size_t>(P) * WcTraits<K, W>::BW * 4 +
-               static_cast<size_t>(P) * 8;
+        return static_cast<size_t>(P) * WcTraits<K, W>::BW * 4 + static_cast<size_t>(P) * 8;
     }
 };
 
-// Scatter of a raw key column (row = key index).
-template <typename K, int THREADS, int V, int W, int NSTAGE>
+// Scatter of a raw key column (row = key index).  V keys per thread per
+// round (whole 16-byte vectors), the next two rounds' vectors loaded while
+// the current round is processed.  Per partition the CTA keeps a W-tuple
+// buffer and a packed {fill, cursor} pair (one 64-bit shared access).
+template <typename K, int THREADS, int V, int W, bool HASHD>
 __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __restrict__ keys, int64_t n,
                                                                   int64_t chunk, int32_t n_items, DigitFn f,
                                                                   int32_t P, const int64_t* __restrict__ offsets,
                                                                   uint32_t* __restrict__ out, uint32_t out_cap,
                                                                   uint32_t* __restrict__ status)
 {
-    using SM = ScatterSmem<K, THREADS, V, W, NSTAGE>;
     constexpr int TW = WcTraits<K, W>::TW, BW = WcTraits<K, W>::BW;
+    constexpr int VN = Vec16<K>::N;
+    constexpr int NV = V / VN;  // vectors per thread per round
+    static_assert(V % VN == 0, "V must be whole vectors");
+    constexpr int ROUND = THREADS * V;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* stages = smem;
-    uint32_t* buf = reinterpret_cast<uint32_t*>(smem + NSTAGE * SM::STAGE_BYTES);
-    int* fill = reinterpret_cast<int*>(buf + static_cast<size_t>(P) * BW);
-    uint32_t* cursor = reinterpret_cast<uint32_t*>(fill + P);
-    __shared__ uint64_t bars[NSTAGE];
-
-    BulkRing<NSTAGE, SM::STAGE_BYTES> ring;
-    ring.stages = stages;
-    ring.bars = bars;
-    ring.phase_bits = 0;
-    ring.init_barriers();
+    uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
+    int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * BW);  // {fill, cursor}
 
     for (int32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-        for (int p = threadIdx.x; p < P; p += THREADS) {
-            fill[p] = 0;
-            cursor[p] = static_cast<uint32_t>(offsets[static_cast<int64_t>(p) * n_items + item]);
-        }
+        for (int p = threadIdx.x; p < P; p += THREADS)
+            fc[p] = make_int2(0, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
         __syncthreads();
         int64_t lo = static_cast<int64_t>(item) * chunk;
         const int64_t hi = lo + chunk < n ? lo + chunk : n;
         if (lo > hi) lo = hi;
-        const int64_t bulk_keys = (((hi - lo) * static_cast<int64_t>(sizeof(K))) & ~int64_t(15)) / sizeof(K);
-        ring.start(keys + lo, bulk_keys * static_cast<int64_t>(sizeof(K)), status);
-        const int64_t nch = ring.num_chunks();
-        const int64_t tail_chunks = (hi - lo - bulk_keys) > 0 ? 1 : 0;
-        for (int64_t c = 0; c < nch + tail_chunks; ++c) {
-            K key[V];
-            int32_t row[V];
-            bool ok[V];
-            uint32_t d[V];
-            int s[V], F[V], Q[V];
-            if (c < nch) {
-                const K* sk = reinterpret_cast<const K*>(ring.wait(c));
-                const int64_t cbase = lo + c * SM::ROUND;
-                const int64_t left = bulk_keys - c * SM::ROUND;
-                const int cnt = left < SM::ROUND ? static_cast<int>(left) : SM::ROUND;
+        const K* kp = keys + lo;
+        const uint32_t len = static_cast<uint32_t>(hi - lo);
+        const uint32_t row0 = static_cast<uint32_t>(lo);
+
+        // element e of vector j of this thread in the round at offset b:
+        //   b + (j * THREADS + threadIdx.x) * VN + e
+        auto load_round = [&](uint32_t b, K (&dst)[NV][VN]) {
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int j = v * THREADS + threadIdx.x;
-                    ok[v] = j < cnt;
-                    key[v] = ok[v] ? sk[j] : K(0);
-                    row[v] = static_cast<int32_t>(cbase + j);
-                    d[v] = ok[v] ? key_digit(f, key[v]) : 0u;
-                }
-            } else {  // the < 16-byte tail the bulk copies leave out
+            for (int j = 0; j < NV; ++j) {
+                const uint32_t at = b + (static_cast<uint32_t>(j) * THREADS + threadIdx.x) * VN;
+                if (at + VN <= len) {
+                    load_vec16<K>(kp + at, dst[j]);
+                } else {
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int64_t j = lo + bulk_keys + v * THREADS + threadIdx.x;
-                    ok[v] = j < hi;
-                    key[v] = ok[v] ? keys[j] : K(0);
-                    row[v] = static_cast<int32_t>(j);
-                    d[v] = ok[v] ? key_digit(f, key[v]) : 0u;
+                    for (int e = 0; e < VN; ++e) dst[j][e] = at + e < len ? kp[at + e] : K(0);
                 }
             }
-            wc_phase_a<K, W, V>(key, row, ok, d, s, buf, fill);
+        };
+        K nxt[NV][VN], nxt2[NV][VN];
+        if (len > 0) load_round(0, nxt);
+        if (ROUND < len) load_round(ROUND, nxt2);
+        for (uint32_t b = 0; b < len; b += ROUND) {
+            K cur[NV][VN];
+#pragma unroll
+            for (int j = 0; j < NV; ++j)
+#pragma unroll
+                for (int e = 0; e < VN; ++e) {
+                    cur[j][e] = nxt[j][e];
+                    nxt[j][e] = nxt2[j][e];
+                }
+            if (b + 2 * ROUND < len) load_round(b + 2 * ROUND, nxt2);
+            const bool full = b + ROUND <= len;
+
+            uint32_t w[V][TW];
+            uint32_t dv[V];  // the tuple's partition
+            int s[V], F[V], Q[V];
+            bool ok[V];
+#pragma unroll
+            for (int j = 0; j < NV; ++j)
+#pragma unroll
+                for (int e = 0; e < VN; ++e) {
+                    const int v = j * VN + e;
+                    const uint32_t at = b + (static_cast<uint32_t>(j) * THREADS + threadIdx.x) * VN + e;
+                    ok[v] = full || at < len;
+                    const K k = cur[j][e];
+                    tuple_words<K>(w[v], k, static_cast<int32_t>(row0 + at));
+                    uint32_t d;
+                    if constexpr (HASHD) {
+                        const uint32_t h = sizeof(K) == 4 ? w[v][0] : hash_key(k);
+                        d = (h >> f.shift) & f.mask;
+                    } else {
+                        d = static_cast<uint32_t>(static_cast<uint64_t>(k) >> f.shift) & f.mask;
+                    }
+                    dv[v] = d;
+                }
+            // phase A
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                s[v] = ok[v] ? atomicAdd(&fc[dv[v]].x, 1) : -1;
+                if (ok[v] && s[v] < W) store_words<TW>(buf + dv[v] * BW + s[v] * TW, w[v]);
+            }
             __syncthreads();
-            if (c < nch) ring.release(c);
-            wc_phase_b<K, W, V>(key, row, ok, d, s, F, Q, buf, fill, cursor, out, out_cap, status);
+            // phase B: only the tuples at or past the buffer's last slot act
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (s[v] >= W - 1) {
+                    const int2 st = fc[dv[v]];
+                    F[v] = st.x;
+                    Q[v] = F[v] & ~(W - 1);
+                    const uint32_t cur_p = static_cast<uint32_t>(st.y);
+                    if (s[v] == W - 1) {
+                        if (cur_p + static_cast<uint32_t>(W) <= out_cap)
+                            wc_flush<K, W>(buf + dv[v] * BW, out + static_cast<size_t>(cur_p) * TW);
+                        else
+                            raise_status(status, ST_INTERNAL);
+                    } else if (s[v] < Q[v]) {
+                        const uint32_t pos = cur_p + static_cast<uint32_t>(s[v]);
+                        if (pos < out_cap)
+                            store_words<TW>(out + static_cast<size_t>(pos) * TW, w[v]);
+                        else
+                            raise_status(status, ST_INTERNAL);
+                    }
+                }
+            }
             __syncthreads();
-            wc_phase_c<K, W, V>(key, row, ok, d, s, F, Q, buf, fill, cursor);
+            // phase C
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (s[v] >= W - 1) {
+                    if (s[v] >= Q[v] && s[v] >= W) store_words<TW>(buf + dv[v] * BW + (s[v] - Q[v]) * TW, w[v]);
+                    if (s[v] == W - 1) {
+                        const int2 st = fc[dv[v]];
+                        fc[dv[v]] = make_int2(F[v] - Q[v], st.y + Q[v]);
+                    }
+                }
+            }
             __syncthreads();
         }
         // final flush: pad every partial buffer to W tuples and write it
         for (int p = threadIdx.x; p < P; p += THREADS) {
-            const int fl = fill[p];
-            uint32_t cur = cursor[p];
+            const int fl = fc[p].x;
+            uint32_t cur_p = static_cast<uint32_t>(fc[p].y);
             if (fl > 0) {
-                uint32_t* b = buf + static_cast<size_t>(p) * BW;
-                for (int q = fl; q < W; ++q) pad_tuple_words<K>(b + q * TW);
-                if (cur + static_cast<uint32_t>(W) <= out_cap)
-                    wc_flush<K, W>(b, out + static_cast<size_t>(cur) * TW);
+                uint32_t* bq = buf + static_cast<size_t>(p) * BW;
+                for (int q = fl; q < W; ++q) {
+                    uint32_t pad[TW];
+#pragma unroll
+                    for (int i = 0; i < TW; ++i) pad[i] = 0u;
+                    pad[TW - 1] = static_cast<uint32_t>(PAD_ROW);
+                    store_words<TW>(bq + q * TW, pad);
+                }
+                if (cur_p + static_cast<uint32_t>(W) <= out_cap)
+                    wc_flush<K, W>(bq, out + static_cast<size_t>(cur_p) * TW);
                 else
                     raise_status(status, ST_INTERNAL);
-                cur += W;
+                cur_p += W;
             }
-            if (cur != static_cast<uint32_t>(offsets[static_cast<int64_t>(p) * n_items + item + 1]))
+            if (cur_p != static_cast<uint32_t>(offsets[static_cast<int64_t>(p) * n_items + item + 1]))
                 raise_status(status, ST_INTERNAL);
         }
         __syncthreads();

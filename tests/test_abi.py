@@ -42,9 +42,9 @@ def test_status_strings(L):
 def test_plan_default_sizes():
     from partitioned_join_b200 import api
     p = api.plan_default(1 << 27, 1 << 27, 4)
-    assert p.passes == 1 and p.table_slots > 0
+    assert p.passes == 1 and p.table_capacity > 0
     # every partition (at the expected size) fits the tables of its splits
-    cap = int(p.table_slots * p.max_fill)
+    cap = p.table_capacity
     assert (1 << 27) / (1 << p.bits1) <= cap * 64
     small = api.plan_default(1000, 4000, 4)
     assert small.bits1 == 0
@@ -69,7 +69,7 @@ def test_invalid_arguments_rejected(L):
     bad.passes = 3
     assert L.pj_workspace_size(ctypes.byref(d), ctypes.byref(bad), ctypes.byref(n)) == _lib.ERR_INVALID
     bad = api.plan_default(100, 100, 4)
-    bad.table_slots = 1 << 30
+    bad.table_capacity = 1 << 30
     assert L.pj_workspace_size(ctypes.byref(d), ctypes.byref(bad), ctypes.byref(n)) == _lib.ERR_INVALID
     # the join refuses a workspace that is missing
     out = _lib.Output()

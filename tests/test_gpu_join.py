@@ -5,7 +5,8 @@ import pytest
 import torch
 
 from oracle import oracle
-from partitioned_join_b200 import DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, PJError
+from partitioned_join_b200 import (DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, TABLE_BUCKET,
+                                   TABLE_OPEN, PJError)
 from partitioned_join_b200 import api, datagen
 
 pytestmark = pytest.mark.gpu
@@ -96,15 +97,17 @@ def test_partition_stage_exact(dtype, bits, mode):
     assert off[0] == 0 and np.all(np.diff(off) >= 0)
     rec = t[: off[-1] * words].reshape(-1, words)
     rows = rec[:, -1]
+    real = rows >= 0
     if dtype == np.int32:
-        k = rec[:, 0].astype(np.int32)
+        # 4-byte keys are stored as murmur(key), a bijection of 32-bit values
+        k = rec[:, 0].astype(np.uint32)
+        assert np.array_equal(k[real], oracle.hash_keys(keys[rows[real]]))
     else:
         k = (rec[:, 1].astype(np.int64) << 32) | (rec[:, 0].astype(np.int64) & 0xFFFFFFFF)
-    real = rows >= 0
+        assert np.array_equal(k[real], keys[rows[real]])
     assert np.all(rows[~real] == -1)
-    # every input row exactly once, carrying its own key
+    # every input row exactly once
     assert np.array_equal(np.sort(rows[real]), np.arange(n))
-    assert np.array_equal(k[real], keys[rows[real]])
     # every row sits in its digit's partition
     part = np.repeat(np.arange(P), np.diff(off))
     d = oracle.digits(keys, mode, bits, 0, 0)
@@ -145,15 +148,30 @@ def test_join_config2_shape_scaled():
 
 
 @pytest.mark.parametrize("digit", [DIGIT_RAW, DIGIT_HASH])
-@pytest.mark.parametrize("slot", [SLOT_FAST, SLOT_REF])
+@pytest.mark.parametrize("table,slot", [(TABLE_BUCKET, SLOT_FAST), (TABLE_OPEN, SLOT_FAST), (TABLE_OPEN, SLOT_REF)])
 @pytest.mark.parametrize("split", [SPLIT_HASH, SPLIT_POSITION])
-def test_join_plan_variants(digit, slot, split):
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+def test_join_plan_variants(digit, table, slot, split, dtype):
     b, p = datagen.config2(seed=13, n_build=300000, n_probe=500000)
-    plan = api.plan_default(b.shape[0], p.shape[0], 4)
-    plan.digit_mode, plan.slot_mode, plan.split_mode = digit, slot, split
-    plan.bits1 = 3                  # coarse: forces 2..8 pieces per partition
-    plan.table_slots = 8192
+    b, p = b.astype(dtype), p.astype(dtype)
+    if dtype == np.int64:
+        b = b * 7919 - (1 << 40)
+        p = p * 7919 - (1 << 40)
+    plan = api.plan_default(b.shape[0], p.shape[0], np.dtype(dtype).itemsize)
+    plan.digit_mode, plan.table_mode, plan.slot_mode, plan.split_mode = digit, table, slot, split
+    plan.bits1 = 3                  # coarse: forces several pieces per partition
+    plan.table_capacity = 8192
     plan.probe_chunk = 4096         # several probe chunks per partition
+    br, pr = run(b, p, True, plan)
+    assert pairs_equal(b, p, br, pr)
+
+
+@pytest.mark.parametrize("w", [2, 4, 8])
+def test_join_wc_widths(w):
+    b, p = datagen.config2(seed=18, n_build=200000, n_probe=300000)
+    plan = api.plan_default(b.shape[0], p.shape[0], 4)
+    plan.wc_tuples = w
+    plan.bits1 = 7
     br, pr = run(b, p, True, plan)
     assert pairs_equal(b, p, br, pr)
 
