@@ -295,10 +295,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 
     __shared__ int64_t s_item, s_next;
     __shared__ uint32_t s_q;                  // entries this CTA produced
-    __shared__ long long s_cbase[OUT_SLOTS];  // output chunk bases
-    __shared__ int s_cid[OUT_SLOTS];          // chunk number held by each slot
+    __shared__ unsigned long long s_cslot[OUT_SLOTS];  // (chunk << 40) | base, ~0: empty
     __shared__ uint32_t s_warp[NWARPS];
     __shared__ int s_nbuild;
+    __shared__ uint32_t s_step;  // next probe step of the current item
 
     const int NB = 1 << a.nb_log2;
     const uint32_t nb_mask = static_cast<uint32_t>(NB - 1);
@@ -309,29 +309,32 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         s_q = 0;
         s_next = static_cast<int64_t>(atomicAdd(a.queue, 1u));
     }
-    if (threadIdx.x < OUT_SLOTS) s_cid[threadIdx.x] = -1;
+    if (threadIdx.x < OUT_SLOTS) s_cslot[threadIdx.x] = ~0ull;
 
     // -- output ------------------------------------------------------------
     // Base of output chunk ch: reserved with one global atomic by the lane
     // whose entries include the chunk's first position, read by the others.
+    // A slot holds (ch << 40) | base in one 64-bit word, so a reader sees a
+    // consistent pair without a memory fence (a fence would wait for the
+    // thread's outstanding global stores).
     auto chunk_base = [&](uint32_t ch, bool reserve) -> long long {
         const int slot = static_cast<int>(ch % OUT_SLOTS);
-        volatile int* vcid = s_cid;
-        volatile long long* vbase = s_cbase;
+        volatile unsigned long long* vslot = s_cslot;
         if (reserve) {
-            const long long g = static_cast<long long>(atomicAdd(a.count, static_cast<unsigned long long>(OUT_CHUNK)));
-            vbase[slot] = g;
-            __threadfence_block();
-            vcid[slot] = static_cast<int>(ch);
-            return g;
+            const unsigned long long g = atomicAdd(a.count, static_cast<unsigned long long>(OUT_CHUNK));
+            vslot[slot] = (static_cast<unsigned long long>(ch) << 40) | g;
+            return static_cast<long long>(g);
         }
         uint32_t spins = 0;
         for (;;) {
-            const int c = vcid[slot];
-            if (c == static_cast<int>(ch)) break;
-            if (c > static_cast<int>(ch)) {  // slot reused: cannot happen with OUT_SLOTS of slack
-                raise_status(a.status, ST_INTERNAL);
-                return -1;
+            const unsigned long long v = vslot[slot];
+            if (v != ~0ull) {
+                const uint32_t c = static_cast<uint32_t>(v >> 40);
+                if (c == ch) return static_cast<long long>(v & ((1ull << 40) - 1));
+                if (c > ch) {  // slot reused: cannot happen with OUT_SLOTS of slack
+                    raise_status(a.status, ST_INTERNAL);
+                    return -1;
+                }
             }
             if (++spins > SPIN_LIMIT) {
                 raise_status(a.status, ST_TIMEOUT);
@@ -339,8 +342,6 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             }
             __nanosleep(20);
         }
-        __threadfence_block();
-        return vbase[slot];
     };
     auto store_out = [&](long long pos, int32_t b, int32_t q) {
         if (pos < a.capacity) {
@@ -376,11 +377,22 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         if (lane == 1 && ch1 != ch0) b1 = chunk_base(ch1, true);  // its first position is ours
         b0 = __shfl_sync(0xffffffffu, b0, 0);
         b1 = __shfl_sync(0xffffffffu, b1, 1);
-        for (int i = lane; i < n; i += 32) {
-            const uint32_t q = q0 + static_cast<uint32_t>(i);
-            const long long base = q / OUT_CHUNK == ch0 ? b0 : b1;
-            if (base >= 0) store_out(base + q % OUT_CHUNK, stage_b[i], stage_p[i]);
+        // entries [0, n0) go to chunk ch0, the rest to ch1
+        const int n0 = ch1 == ch0 ? n : static_cast<int>(ch1 * OUT_CHUNK - q0);
+        const uint32_t off0 = q0 % OUT_CHUNK;
+        if (b0 >= 0 && b0 + off0 + n0 <= a.capacity) {
+            int32_t* ob = a.out_build + b0 + off0;
+            int32_t* op = a.out_probe + b0 + off0;
+            for (int i = lane; i < n0; i += 32) {
+                ob[i] = stage_b[i];
+                op[i] = stage_p[i];
+            }
+        } else {
+            for (int i = lane; i < n0; i += 32)
+                if (b0 >= 0) store_out(b0 + off0 + i, stage_b[i], stage_p[i]);
         }
+        for (int i = n0 + lane; i < n; i += 32)
+            if (b1 >= 0) store_out(b1 + (i - n0), stage_b[i], stage_p[i]);
         __syncwarp();
     };
 
@@ -430,6 +442,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         auto slot_of = [&](uint32_t h) -> uint32_t {
             return SLOT_REF ? slot_ref(h, a.cap) : slot_fast(h, skip, static_cast<uint32_t>(a.cap));
         };
+
+        if (threadIdx.x == 0) s_step = 0;  // ordered before the probe by the build's barriers
 
         // ---- build ----
         bool skip_item = false;
@@ -545,21 +559,30 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 
         // ---- probe: warps run independently; loads run one step ahead ----
         if (!skip_item) {
-            const int64_t per_step = static_cast<int64_t>(NWARPS) * 32 * U;
+            // warps claim steps of 32*U tuples from a shared counter, so they
+            // finish the item together; the next claim's loads run ahead
+            const uint32_t* pbase = a.probe_tuples + q_lo * TV::WORDS;
+            const uint32_t qn = static_cast<uint32_t>(q_hi - q_lo);
+            constexpr uint32_t STEP = 32 * U;
             uint32_t nh[U];
             Cmp nk[U];
             int32_t nr[U];
-            auto load_step = [&](int64_t s0) {
+            auto claim = [&]() -> uint32_t {
+                uint32_t st = 0;
+                if (lane == 0) st = atomicAdd(&s_step, 1u);
+                return __shfl_sync(0xffffffffu, st, 0) * STEP;
+            };
+            auto load_step = [&](uint32_t s0) {
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    const int64_t i = s0 + u * 32 + lane;
+                    const uint32_t i = s0 + u * 32 + lane;
                     nr[u] = -1;
-                    if (i < q_hi) TV::load(a.probe_tuples, i, nh[u], nk[u], nr[u]);
+                    if (i < qn) TV::load(pbase, i, nh[u], nk[u], nr[u]);
                 }
             };
-            int64_t s0 = q_lo + static_cast<int64_t>(warp) * 32 * U;
-            if (s0 < q_hi) load_step(s0);
-            for (; s0 < q_hi; s0 += per_step) {
+            uint32_t s0 = claim();
+            if (s0 < qn) load_step(s0);
+            while (s0 < qn) {
                 uint32_t h[U];
                 Cmp k[U];
                 int32_t r[U];
@@ -569,7 +592,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                     k[u] = nk[u];
                     r[u] = nr[u];
                 }
-                if (s0 + per_step < q_hi) load_step(s0 + per_step);
+                const uint32_t s_after = claim();
+                if (s_after < qn) load_step(s_after);
                 // look up one tuple from (at, end) or slot sl; returns whether a match was found
                 auto lookup = [&](int u, int& at_u, int end_u, uint32_t& sl_u, int& steps_u, bool& live_u,
                                   uint32_t& brow_u) -> bool {
@@ -621,7 +645,61 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         sl_u = slot_of(h[u]);
                     }
                 };
-                if constexpr (UNIQUE) {
+                if constexpr (UNIQUE && TABLE == TABLE_BUCKET) {
+                    // every tuple matches at most once.  The U tuples walk their
+                    // buckets in lockstep so their shared loads overlap.
+                    bool emit[U], live[U];
+                    uint32_t brow[U];
+                    int at[U], end[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        emit[u] = false;
+                        brow[u] = 0;
+                        live[u] = r[u] >= 0 && in_piece(h[u]);
+                        at[u] = end[u] = 0;
+                        if (live[u]) {
+                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t wb = ends[b >> 1];
+                            const uint32_t wa = b == 0 ? 0u : ends[(b - 1) >> 1];
+                            end[u] = static_cast<int>((wb >> ((b & 1u) * 16)) & 0xffffu);
+                            at[u] = b == 0 ? 0 : static_cast<int>((wa >> (((b - 1) & 1u) * 16)) & 0xffffu);
+                            live[u] = at[u] < end[u];
+                        }
+                    }
+                    for (;;) {
+                        bool any = false;
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            if (live[u]) {
+                                Cmp ek;
+                                uint32_t er;
+                                E::get(table, at[u], ek, er);
+                                ++at[u];
+                                if (ek == k[u]) {
+                                    emit[u] = true;
+                                    brow[u] = er;
+                                    live[u] = false;
+                                } else {
+                                    live[u] = at[u] < end[u];
+                                }
+                            }
+                            any |= live[u];
+                        }
+                        if (!any) break;
+                    }
+                    int c = 0;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) c += emit[u] ? 1 : 0;
+                    append(c, [&](int at_stage) {
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+                            if (emit[u]) {
+                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
+                                stage_p[at_stage] = r[u];
+                                ++at_stage;
+                            }
+                    });
+                } else if constexpr (UNIQUE) {
                     // every tuple matches at most once: one lookup, one append per warp step
                     bool emit[U];
                     uint32_t brow[U];
@@ -682,6 +760,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         if (!__any_sync(0xffffffffu, any_live)) break;
                     }
                 }
+                s0 = s_after;
             }
         }
     }
@@ -690,7 +769,9 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     if (threadIdx.x == 0) {
         const uint32_t q = s_q;
         a.cta_q[blockIdx.x] = q;
-        a.cta_last[blockIdx.x] = (q > 0 && write_out) ? s_cbase[((q - 1) / OUT_CHUNK) % OUT_SLOTS] : -1;
+        a.cta_last[blockIdx.x] =
+            (q > 0 && write_out) ? static_cast<int64_t>(s_cslot[((q - 1) / OUT_CHUNK) % OUT_SLOTS] & ((1ull << 40) - 1))
+                                 : -1;
     }
 }
 
