@@ -170,6 +170,15 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     return PJ_OK;
 }
 
+// Resident join CTAs per SM for this plan: shared memory and threads bound it.
+int join_ctas_per_sm(int key_bytes, const pj_plan* p)
+{
+    const size_t smem = join_smem(key_bytes, p->table_mode, p->table_capacity);
+    const int by_smem = static_cast<int>((smem_limit() + 1024) / std::max<size_t>(smem + 1024, 1));
+    const int by_threads = 2048 / JN_THREADS;
+    return std::max(1, std::min({MAX_JOIN_CTAS_PER_SM, by_smem, by_threads}));
+}
+
 // Build tuples one table holds.
 int table_tuples(const pj_plan* p)
 {
@@ -249,7 +258,7 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.item_part = take(4 * static_cast<size_t>(L.max_items));
     // output fix-up: per join CTA records, segments, and room for the
     // reserved positions past the caller's capacity (one chunk per CTA)
-    L.max_ctas = sm_count() * MAX_JOIN_CTAS_PER_SM;
+    L.max_ctas = sm_count() * join_ctas_per_sm(d->key_bytes, p);
     L.over_cap = static_cast<int64_t>(L.max_ctas) * OUT_CHUNK;
     L.cta_q = take(8 * static_cast<size_t>(L.max_ctas));
     L.cta_last = take(8 * static_cast<size_t>(L.max_ctas));
@@ -402,7 +411,7 @@ pj_status launch_join_t(const JoinArgs& a, cudaStream_t st)
     int per_sm = 0;
     PJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, JN_THREADS, smem));
     per_sm = std::min(std::max(per_sm, 1), MAX_JOIN_CTAS_PER_SM);
-    const int grid = sm_count() * per_sm;
+    const int grid = std::min(sm_count() * per_sm, a.max_ctas);
     kern<<<grid, JN_THREADS, smem, st>>>(a);
     PJ_CUDA(cudaGetLastError());
     // fix-up: dense output and the true count
@@ -545,6 +554,7 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     a.over_build = reinterpret_cast<int32_t*>(ws + L.over_b);
     a.over_probe = reinterpret_cast<int32_t*>(ws + L.over_p);
     a.over_cap = L.over_cap;
+    a.max_ctas = L.max_ctas;
     E.mark(PJ_STAGE_JOIN, st);
     s = launch_join<K>(a, p->table_mode, d->unique_build_keys != 0, hash_split, p->slot_mode == PJ_SLOT_REF, st);
     E.mark(PJ_STAGE_TOTAL, st);

@@ -75,6 +75,7 @@ struct JoinArgs {
     int32_t* over_probe;
     int64_t over_cap;
     int64_t* seg;               // fix-up segments
+    int32_t max_ctas;           // join CTAs the fix-up records have room for
 };
 
 // Items per partition (S_p x K_p) and the split of partition p.
