@@ -193,6 +193,28 @@ pj_status pj_inner_join_events(const pj_join_desc* desc, const pj_plan* plan, pj
  * PJ_ERR_TIMEOUT or PJ_ERR_INTERNAL), then clears it. */
 pj_status pj_check(void* workspace, pj_stream stream);
 
+/* Size of the library's built-in workspace on each device (64 MiB). */
+#define PJ_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* pj_inner_join for callers that cannot allocate device memory: no
+ * counterpart in the reference, which allocates its buffers itself.  The
+ * workspace is a fixed array of PJ_NOALLOC_SCRATCH_BYTES inside the library,
+ * one per device, so a caller passes only its key and output columns.  Meant
+ * for hosts that bind the join through an FFI without a device allocator, and
+ * for callers that must avoid cudaMalloc/cudaFree (cudaFree waits for the
+ * whole device).
+ * - Joins whose pj_workspace_size() exceeds PJ_NOALLOC_SCRATCH_BYTES (about
+ *   2^20 x 2^22 4-byte keys with the default plan) return PJ_ERR_WORKSPACE
+ *   before any device work; use pj_inner_join for them.
+ * - The first call on each device sets up the array's address (and loads its
+ *   module); make it before any stream capture on that device.
+ * - Nothing has to be zeroed beforehand: every call clears what it uses.
+ * - SYNCHRONISES the stream and returns the final status (that of pj_check).
+ * - Calls that overlap in time on one device share the array and race:
+ *   serialise them. */
+pj_status pj_inner_join_noalloc(const pj_join_desc* desc, const pj_plan* plan, pj_output* out,
+                                pj_stream stream);
+
 /* ---- stage entry points (each replaces one reference stage) ------------- */
 
 /* MurmurHash3_32 (seed 0) of every key: MurmurHash3_32<K>::operator(),

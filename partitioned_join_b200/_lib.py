@@ -14,6 +14,7 @@ DIGIT_RAW, DIGIT_HASH = 0, 1
 SLOT_FAST, SLOT_REF = 0, 1
 SPLIT_HASH, SPLIT_POSITION = 0, 1
 TABLE_BUCKET, TABLE_OPEN = 0, 1
+NOALLOC_SCRATCH_BYTES = 64 << 20  # PJ_NOALLOC_SCRATCH_BYTES
 STAGES = ["build_hist", "build_scan", "build_scatter", "probe_hist", "probe_scan", "probe_scatter", "join_plan",
           "join", "total"]
 
@@ -61,6 +62,7 @@ SIGNATURES = {
                                             _SZ, _P, ctypes.POINTER(ctypes.c_void_p)]),
     "pj_join_count": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), _P, _P, _SZ, _P]),
     "pj_check": (ctypes.c_int, [_P, _P]),
+    "pj_inner_join_noalloc": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), ctypes.POINTER(Output), _P]),
     "pj_hash_keys": (ctypes.c_int, [_P, _I64, _I32, _P, _P]),
     "pj_hash_slots": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _P, _P]),
     "pj_radix_histogram": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _I32, _P, _P]),

@@ -183,6 +183,30 @@ def partitioned_join(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_
     return j.result(stream)
 
 
+def inner_join_noalloc(build_keys: torch.Tensor, probe_keys: torch.Tensor, capacity: int,
+                       unique_build_keys: bool = True, plan: Optional[Plan] = None,
+                       stream=None) -> Tuple[torch.Tensor, torch.Tensor]:
+    """The join through pj_inner_join_noalloc: the library uses its built-in
+    64 MiB workspace instead of one allocated here, so only the output
+    columns (capacity pairs) are allocated by the caller.  Raises PJError
+    (workspace) for joins too large for that workspace.  Synchronises the
+    stream."""
+    b = _keys(build_keys, "build_keys")
+    p = _keys(probe_keys, "probe_keys")
+    desc = make_desc(b, p, unique_build_keys)
+    dev = b.device
+    build_row = torch.empty(max(capacity, 1), dtype=torch.int32, device=dev)
+    probe_row = torch.empty(max(capacity, 1), dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    out = Output()
+    out.build_row, out.probe_row = build_row.data_ptr(), probe_row.data_ptr()
+    out.capacity, out.count = capacity, count.data_ptr()
+    check(lib().pj_inner_join_noalloc(ctypes.byref(desc), ctypes.byref(plan) if plan is not None else None,
+                                      ctypes.byref(out), _stream_ptr(stream)), "pj_inner_join_noalloc")
+    n = int(count.item())
+    return build_row[:n], probe_row[:n]
+
+
 def join_count(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_keys: bool = True,
                plan: Optional[Plan] = None) -> int:
     d = make_desc(build_keys, probe_keys, unique_build_keys)
