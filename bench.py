@@ -35,15 +35,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "tuples/s & HBM-roofline %, 2^27x2^27 int32 join"
 # kernels of one pj_inner_join: per side histogram, scan, scatter; then
-# join_items, scan, items_expand, join
-LAUNCHES_PER_JOIN = 10
+# join_items, scan, items_expand, join, fix-up plan, fix-up move
+LAUNCHES_PER_JOIN = 12
 UNIT = "tuples/s"
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--log2-build", type=int, default=27)
