@@ -115,6 +115,12 @@ class ClockSampler:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver queries) must not overlap the timed
+        # region: wait for its first sample
+        t_end = time.time() + 10
+        while time.time() < t_end and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
