@@ -101,8 +101,11 @@ typedef struct pj_output {
 /* Shared-memory table of the join. */
 enum {
     PJ_TABLE_BUCKET = 0,  /* build tuples counting-sorted by hash bucket (8 B a tuple) */
-    PJ_TABLE_OPEN = 1     /* the reference's open addressing, linear probing,
+    PJ_TABLE_OPEN = 1,    /* the reference's open addressing, linear probing,
                              hash_join_kernels.cuh:19-129 */
+    PJ_TABLE_COMPACT = 2  /* bucket order with 4-byte entries (hash fingerprint and
+                             index of the build tuple): ~2x the tuples per table;
+                             a build range must stay within 65536 tuples */
 };
 
 /* Execution plan.  pj_plan_default() fills it from the sizes alone,

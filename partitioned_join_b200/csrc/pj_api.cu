@@ -112,19 +112,25 @@ bool sector_wc(int key_bytes, int W) { return valid_wc(key_bytes, W) && (W * tup
 
 int bucket_nb_log2(int cap) { return std::max(1, ilog2_floor(std::max(2, cap / 2))); }
 
-size_t join_smem(int key_bytes, int table_mode, int cap)
+template <typename K>
+size_t join_smem_k(int table_mode, int cap)
 {
     const int nb = bucket_nb_log2(cap);
-    if (key_bytes == 4)
-        return table_mode == PJ_TABLE_BUCKET ? JoinSmem<int32_t, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS)
-                                             : JoinSmem<int32_t, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
-    return table_mode == PJ_TABLE_BUCKET ? JoinSmem<int64_t, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS)
-                                         : JoinSmem<int64_t, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
+    switch (table_mode) {
+    case PJ_TABLE_BUCKET: return JoinSmem<K, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS);
+    case PJ_TABLE_COMPACT: return JoinSmem<K, TABLE_COMPACT>::bytes(cap, nb, JN_THREADS);
+    default: return JoinSmem<K, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
+    }
+}
+
+size_t join_smem(int key_bytes, int table_mode, int cap)
+{
+    return key_bytes == 4 ? join_smem_k<int32_t>(table_mode, cap) : join_smem_k<int64_t>(table_mode, cap);
 }
 
 int max_table_capacity(int key_bytes, int table_mode)
 {
-    int lo = 64, hi = table_mode == PJ_TABLE_BUCKET ? MAX_BUCKET_CAP : (1 << 20);
+    int lo = 64, hi = table_mode == PJ_TABLE_OPEN ? (1 << 20) : MAX_BUCKET_CAP;
     const size_t lim = smem_limit();
     if (join_smem(key_bytes, table_mode, lo) > lim) return 0;
     while (lo < hi) {  // largest cap that fits
@@ -154,7 +160,8 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (!valid_wc(d->key_bytes, p->wc_tuples)) return PJ_ERR_INVALID;
     if (scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) > smem_limit()) return PJ_ERR_INVALID;
     if (p->digit_mode != PJ_DIGIT_RAW && p->digit_mode != PJ_DIGIT_HASH) return PJ_ERR_INVALID;
-    if (p->table_mode != PJ_TABLE_BUCKET && p->table_mode != PJ_TABLE_OPEN) return PJ_ERR_INVALID;
+    if (p->table_mode != PJ_TABLE_BUCKET && p->table_mode != PJ_TABLE_OPEN && p->table_mode != PJ_TABLE_COMPACT)
+        return PJ_ERR_INVALID;
     if (p->slot_mode != PJ_SLOT_FAST && p->slot_mode != PJ_SLOT_REF) return PJ_ERR_INVALID;
     if (p->split_mode != PJ_SPLIT_HASH && p->split_mode != PJ_SPLIT_POSITION) return PJ_ERR_INVALID;
     if (p->table_capacity < 64 || p->table_capacity > max_table_capacity(d->key_bytes, p->table_mode))
@@ -165,7 +172,7 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (p->table_mode == PJ_TABLE_OPEN && !(p->max_fill > 0.05f && p->max_fill <= 0.95f)) return PJ_ERR_INVALID;
     // hash bits: digits + hash split + bucket/slot bits must fit 32
     const int digit_bits = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0;
-    const int slot_bits = p->table_mode == PJ_TABLE_BUCKET ? bucket_nb_log2(p->table_capacity) : 12;
+    const int slot_bits = p->table_mode != PJ_TABLE_OPEN ? bucket_nb_log2(p->table_capacity) : 12;
     if (digit_bits + MAX_SPLIT_LOG2 + slot_bits > 32) return PJ_ERR_INVALID;
     return PJ_OK;
 }
@@ -182,8 +189,8 @@ int join_ctas_per_sm(int key_bytes, const pj_plan* p)
 // Build tuples one table holds.
 int table_tuples(const pj_plan* p)
 {
-    return p->table_mode == PJ_TABLE_BUCKET ? p->table_capacity
-                                            : std::max(1, static_cast<int>(p->table_capacity * p->max_fill));
+    return p->table_mode != PJ_TABLE_OPEN ? p->table_capacity
+                                          : std::max(1, static_cast<int>(p->table_capacity * p->max_fill));
 }
 
 // ---------------------------------------------------------------------------
@@ -447,6 +454,7 @@ template <typename K>
 pj_status launch_join(const JoinArgs& a, int table_mode, bool unique, bool hash_split, bool slot_ref, cudaStream_t st)
 {
     if (table_mode == PJ_TABLE_BUCKET) return launch_join_tab<K, TABLE_BUCKET>(a, unique, hash_split, false, st);
+    if (table_mode == PJ_TABLE_COMPACT) return launch_join_tab<K, TABLE_COMPACT>(a, unique, hash_split, false, st);
     return launch_join_tab<K, TABLE_OPEN>(a, unique, hash_split, slot_ref, st);
 }
 
@@ -646,18 +654,32 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     p->probe_chunk = 1 << 16;
     p->scatter_ctas_per_sm = 1;
     p->hist_split = 2;
-    // Fewest partitions whose expected build side fills at most 7/8 of a table.
-    const int64_t target = std::max<int64_t>(1, p->table_capacity - p->table_capacity / 8);
-    int bits = ilog2_ceil(std::max<int64_t>(1, (d->n_build + target - 1) / target));
-    // Widest write-combining buffer that the shared memory allows at that fan-out.
+    // Widest write-combining buffer that the shared memory allows at a fan-out.
     auto pick_w = [&](int b) {
         for (int W : {8, 4})
             if (sector_wc(d->key_bytes, W) && scatter_smem(d->key_bytes, W, 1 << b) <= smem_limit() &&
-                (W <= 4 || b <= 8))
+                (W <= 4 || b <= 8 || d->key_bytes == 8))
                 return W;
         return 0;
     };
-    while (bits > 0 && pick_w(bits) == 0) --bits;  // beyond one pass: hash splits absorb the rest
+    // Fewest partitions whose expected build side fills at most 7/8 of a table.
+    auto bits_for = [&](int64_t cap) {
+        const int64_t target = std::max<int64_t>(1, cap - cap / 8);
+        return ilog2_ceil(std::max<int64_t>(1, (d->n_build + target - 1) / target));
+    };
+    int bits = bits_for(p->table_capacity);
+    if (pick_w(bits) == 0) {
+        // beyond one pass's fan-out: 4-byte COMPACT entries hold twice the
+        // tuples per table, so large partitions need no split
+        const int ccap = max_table_capacity(d->key_bytes, PJ_TABLE_COMPACT);
+        // (only where partitions stay within an entry's 16-bit index)
+        if (ccap > p->table_capacity && pick_w(bits_for(ccap)) != 0) {
+            p->table_mode = PJ_TABLE_COMPACT;
+            p->table_capacity = ccap;
+            bits = bits_for(ccap);
+        }
+    }
+    while (bits > 0 && pick_w(bits) == 0) --bits;  // still beyond: hash splits absorb the rest
     p->bits1 = bits;
     p->wc_tuples = pick_w(bits);
     if (p->wc_tuples == 0) p->wc_tuples = d->key_bytes == 4 ? 4 : 8;
@@ -909,6 +931,12 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
     // when their largest partition is no worse than the hashed one's.
     p.digit_mode = raw_max <= hash_max ? PJ_DIGIT_RAW : PJ_DIGIT_HASH;
     const int64_t mx = std::min(raw_max, hash_max);
+    // a COMPACT entry addresses 65536 tuples of a build range (padding included)
+    if (p.table_mode == PJ_TABLE_COMPACT &&
+        mx + static_cast<int64_t>(L.b_items) * (p.wc_tuples - 1) > COMPACT_RANGE) {
+        p.table_mode = PJ_TABLE_BUCKET;
+        p.table_capacity = max_table_capacity(d->key_bytes, PJ_TABLE_BUCKET);
+    }
     const int64_t cap = table_tuples(&p);
     // Hash splits cannot separate repeated keys: a partition beyond what
     // 2^MAX_SPLIT_LOG2 tables hold (duplicates) takes the position split.

@@ -18,7 +18,13 @@
 //   BUCKET (default): the piece's build tuples sorted by bucket = low hash
 //     bits, plus an array of bucket ends (16-bit, two per word).  Built by a
 //     counting sort: count pass, block scan, place pass.  8 bytes a tuple for
-//     4-byte keys, so one CTA holds ~18 K tuples.
+//     4-byte keys, so one CTA holds ~22 K tuples.
+//   COMPACT: the same bucket order, but an entry is 4 bytes: 16 bits of the
+//     hash above the bucket bits (a fingerprint) and the tuple's 16-bit
+//     index in the item's build range.  One CTA holds ~41 K tuples, so large
+//     partitions need no split; a fingerprint hit loads the build tuple
+//     (from L2: the item read it moments before) to compare the full key
+//     and take its row.
 //   OPEN: the reference's layout -- open addressing with linear probing,
 //     fill <= 0.5 (HASH_TABLE_OCC, hash_join_kernels.cuh:21), slot
 //     abs((int)h % T) (:100-101) or a multiply-high of unused hash bits;
@@ -44,7 +50,8 @@
 namespace pj {
 
 constexpr uint32_t EMPTY_ROW = 0xffffffffu;
-enum : int { TABLE_BUCKET = 0, TABLE_OPEN = 1 };
+enum : int { TABLE_BUCKET = 0, TABLE_OPEN = 1, TABLE_COMPACT = 2 };
+constexpr int64_t COMPACT_RANGE = 65536;  // build range a COMPACT entry's index can address
 
 struct JoinArgs {
     const uint32_t* build_tuples;
@@ -144,6 +151,12 @@ template <> struct TupleView<int32_t> {
         key = v.x;
         row = static_cast<int32_t>(v.y);
     }
+    __device__ __forceinline__ static void load_key_row(const uint32_t* base, int64_t i, Cmp& key, int32_t& row)
+    {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(base) + i);
+        key = v.x;
+        row = static_cast<int32_t>(v.y);
+    }
 };
 
 template <> struct TupleView<int64_t> {
@@ -156,6 +169,12 @@ template <> struct TupleView<int64_t> {
         key = (static_cast<unsigned long long>(hi) << 32) | lo;
         row = static_cast<int32_t>(__ldg(p + 2));
         h = hash_key(static_cast<int64_t>(key));
+    }
+    __device__ __forceinline__ static void load_key_row(const uint32_t* base, int64_t i, Cmp& key, int32_t& row)
+    {
+        const uint32_t* p = base + 3 * i;
+        key = (static_cast<unsigned long long>(__ldg(p + 1)) << 32) | __ldg(p);
+        row = static_cast<int32_t>(__ldg(p + 2));
     }
 };
 
@@ -214,13 +233,13 @@ struct JoinSmem {
     // table bytes for capacity cap (BUCKET: tuples; OPEN: slots) and 2^nb_log2 buckets
     __host__ __device__ static size_t entries_bytes(int cap)
     {
-        const size_t e = TABLE == TABLE_OPEN ? (sizeof(K) == 4 ? 8 : 12) : Entry<K>::BYTES;
+        const size_t e = TABLE == TABLE_OPEN ? (sizeof(K) == 4 ? 8 : 12) : TABLE == TABLE_COMPACT ? 4 : Entry<K>::BYTES;
         return (static_cast<size_t>(cap) * e + 127) & ~size_t(127);
     }
     __host__ __device__ static size_t table_bytes(int cap, int nb_log2)
     {
         size_t t = entries_bytes(cap);
-        if (TABLE == TABLE_BUCKET) t += ((static_cast<size_t>(1) << nb_log2) / 2) * 4;
+        if (TABLE != TABLE_OPEN) t += ((static_cast<size_t>(1) << nb_log2) / 2) * 4;
         return (t + 127) & ~size_t(127);
     }
     // plus per-warp staging of 32 * JOIN_U entries (build and probe rows)
@@ -292,6 +311,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     int32_t* stage_p = stage_b + STAGE;
     // OPEN tables of 8-byte keys: keys[cap] (8 B) then rows[cap]
     unsigned long long* okeys = reinterpret_cast<unsigned long long*>(table);
+    uint32_t* ctab = reinterpret_cast<uint32_t*>(table);  // COMPACT: fingerprint << 16 | index
     uint32_t* orows = reinterpret_cast<uint32_t*>(table + static_cast<size_t>(a.cap) * 8);
 
     __shared__ int64_t s_item, s_next;
@@ -440,6 +460,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             return static_cast<int64_t>((h << a.digit_bits) >> piece_shift) == piece;
         };
         auto bucket_of = [&](uint32_t h) -> uint32_t { return h & nb_mask; };
+        auto finger_of = [&](uint32_t h) -> uint32_t { return (h >> a.nb_log2) & 0xffffu; };
         auto slot_of = [&](uint32_t h) -> uint32_t {
             return SLOT_REF ? slot_ref(h, a.cap) : slot_fast(h, skip, static_cast<uint32_t>(a.cap));
         };
@@ -448,7 +469,12 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 
         // ---- build ----
         bool skip_item = false;
-        if constexpr (TABLE == TABLE_BUCKET) {
+        if (TABLE == TABLE_COMPACT && b_hi - b_lo > COMPACT_RANGE) {
+            // an entry's 16-bit index cannot address this range: the planner avoids it
+            if (threadIdx.x == 0) raise_status(a.status, ST_OVERFLOW);
+            skip_item = true;
+            __syncthreads();
+        } else if constexpr (TABLE != TABLE_OPEN) {
             for (int i = threadIdx.x; i < NB / 2; i += THREADS) ends[i] = 0u;
             if (threadIdx.x == 0) s_nbuild = 0;
             __syncthreads();
@@ -513,7 +539,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             const uint32_t b = bucket_of(h[u]);
                             const uint32_t old = atomicAdd(&ends[b >> 1], (b & 1u) ? 0x10000u : 1u);
                             const int pos = static_cast<int>((b & 1u) ? (old >> 16) : (old & 0xffffu));
-                            E::put(table, pos, k[u], r[u]);
+                            if constexpr (TABLE == TABLE_COMPACT)
+                                ctab[pos] = (finger_of(h[u]) << 16) | static_cast<uint32_t>(i0 + u * THREADS - b_lo);
+                            else
+                                E::put(table, pos, k[u], r[u]);
                         }
                     }
                 }
@@ -599,7 +628,24 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                 auto lookup = [&](int u, int& at_u, int end_u, uint32_t& sl_u, int& steps_u, bool& live_u,
                                   uint32_t& brow_u) -> bool {
                     bool found = false;
-                    if constexpr (TABLE == TABLE_BUCKET) {
+                    if constexpr (TABLE == TABLE_COMPACT) {
+                        const uint32_t fq = finger_of(h[u]);
+                        while (at_u < end_u) {
+                            const uint32_t e = ctab[at_u];
+                            ++at_u;
+                            if ((e >> 16) == fq) {  // fingerprint hit: compare the full key
+                                Cmp bk;
+                                int32_t br;
+                                TV::load_key_row(a.build_tuples, b_lo + (e & 0xffffu), bk, br);
+                                if (bk == k[u]) {
+                                    found = true;
+                                    brow_u = static_cast<uint32_t>(br);
+                                    break;
+                                }
+                            }
+                        }
+                        if (!found || UNIQUE) live_u = false;
+                    } else if constexpr (TABLE == TABLE_BUCKET) {
                         while (at_u < end_u) {
                             Cmp ek;
                             uint32_t er;
@@ -638,7 +684,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                     return found;
                 };
                 auto start = [&](int u, int& at_u, int& end_u, uint32_t& sl_u) {
-                    if constexpr (TABLE == TABLE_BUCKET) {
+                    if constexpr (TABLE != TABLE_OPEN) {
                         const uint32_t b = bucket_of(h[u]);
                         end_u = static_cast<int>((ends[b >> 1] >> ((b & 1u) * 16)) & 0xffffu);
                         at_u = b == 0 ? 0 : static_cast<int>((ends[(b - 1) >> 1] >> (((b - 1) & 1u) * 16)) & 0xffffu);
@@ -646,7 +692,81 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         sl_u = slot_of(h[u]);
                     }
                 };
-                if constexpr (UNIQUE && TABLE == TABLE_BUCKET) {
+                if constexpr (UNIQUE && TABLE == TABLE_COMPACT) {
+                    // every tuple matches at most once.  The U tuples walk their
+                    // buckets in lockstep comparing fingerprints; hits load their
+                    // build tuples together; a false hit (equal fingerprint, other
+                    // key) resumes its walk.
+                    bool emit[U], live[U];
+                    uint32_t brow[U], fq[U];
+                    int at[U], end[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        emit[u] = false;
+                        brow[u] = 0;
+                        fq[u] = finger_of(h[u]);
+                        live[u] = r[u] >= 0 && in_piece(h[u]);
+                        at[u] = end[u] = 0;
+                        if (live[u]) {
+                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t wb = ends[b >> 1];
+                            const uint32_t wa = b == 0 ? 0u : ends[(b - 1) >> 1];
+                            end[u] = static_cast<int>((wb >> ((b & 1u) * 16)) & 0xffffu);
+                            at[u] = b == 0 ? 0 : static_cast<int>((wa >> (((b - 1) & 1u) * 16)) & 0xffffu);
+                            live[u] = at[u] < end[u];
+                        }
+                    }
+                    for (;;) {
+                        bool hit[U];
+#pragma unroll
+                        for (int u = 0; u < U; ++u) hit[u] = false;
+                        for (;;) {
+                            bool any = false;
+#pragma unroll
+                            for (int u = 0; u < U; ++u) {
+                                if (live[u]) {
+                                    if ((ctab[at[u]] >> 16) == fq[u]) {
+                                        hit[u] = true;
+                                        live[u] = false;
+                                    } else {
+                                        live[u] = ++at[u] < end[u];
+                                    }
+                                }
+                                any |= live[u];
+                            }
+                            if (!any) break;
+                        }
+                        bool again = false;
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            if (hit[u]) {
+                                Cmp bk;
+                                int32_t br;
+                                TV::load_key_row(a.build_tuples, b_lo + (ctab[at[u]] & 0xffffu), bk, br);
+                                if (bk == k[u]) {
+                                    emit[u] = true;
+                                    brow[u] = static_cast<uint32_t>(br);
+                                } else {
+                                    live[u] = ++at[u] < end[u];
+                                    again |= live[u];
+                                }
+                            }
+                        }
+                        if (!__any_sync(0xffffffffu, again)) break;
+                    }
+                    int c = 0;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) c += emit[u] ? 1 : 0;
+                    append(c, [&](int at_stage) {
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+                            if (emit[u]) {
+                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
+                                stage_p[at_stage] = r[u];
+                                ++at_stage;
+                            }
+                    });
+                } else if constexpr (UNIQUE && TABLE == TABLE_BUCKET) {
                     // every tuple matches at most once.  The U tuples walk their
                     // buckets in lockstep so their shared loads overlap.
                     bool emit[U], live[U];

@@ -6,7 +6,7 @@ import torch
 
 from oracle import oracle
 from partitioned_join_b200 import (DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, TABLE_BUCKET,
-                                   TABLE_OPEN, PJError)
+                                   TABLE_COMPACT, TABLE_OPEN, PJError)
 from partitioned_join_b200 import api, datagen
 
 pytestmark = pytest.mark.gpu
@@ -148,7 +148,8 @@ def test_join_config2_shape_scaled():
 
 
 @pytest.mark.parametrize("digit", [DIGIT_RAW, DIGIT_HASH])
-@pytest.mark.parametrize("table,slot", [(TABLE_BUCKET, SLOT_FAST), (TABLE_OPEN, SLOT_FAST), (TABLE_OPEN, SLOT_REF)])
+@pytest.mark.parametrize("table,slot", [(TABLE_BUCKET, SLOT_FAST), (TABLE_COMPACT, SLOT_FAST), (TABLE_OPEN, SLOT_FAST),
+                                        (TABLE_OPEN, SLOT_REF)])
 @pytest.mark.parametrize("split", [SPLIT_HASH, SPLIT_POSITION])
 @pytest.mark.parametrize("dtype", [np.int32, np.int64])
 def test_join_plan_variants(digit, table, slot, split, dtype):
@@ -162,6 +163,64 @@ def test_join_plan_variants(digit, table, slot, split, dtype):
     plan.bits1 = 3                  # coarse: forces several pieces per partition
     plan.table_capacity = 8192
     plan.probe_chunk = 4096         # several probe chunks per partition
+    br, pr = run(b, p, True, plan)
+    assert pairs_equal(b, p, br, pr)
+
+
+def _fingerprint_twins(dtype, n_pairs, bits=23):
+    """Pairs of distinct keys whose hashes agree on the low `bits` bits."""
+    keys = (np.arange(1, 1 << 22, dtype=np.int64) * 2654435761 + 12345).astype(dtype)
+    low = oracle.hash_keys(keys).astype(np.int64) & ((1 << bits) - 1)
+    order = np.argsort(low, kind="stable")
+    ls = low[order]
+    same = np.nonzero(ls[1:] == ls[:-1])[0]
+    a, b = keys[order[same]], keys[order[same + 1]]
+    # one pair per low value, pairs disjoint
+    _, first = np.unique(ls[same], return_index=True)
+    a, b = a[first], b[first]
+    used = set()
+    pa, pb = [], []
+    for x, y in zip(a.tolist(), b.tolist()):
+        if x in used or y in used:
+            continue
+        used.update((x, y))
+        pa.append(x)
+        pb.append(y)
+        if len(pa) == n_pairs:
+            break
+    return np.array(pa, dtype=dtype), np.array(pb, dtype=dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+@pytest.mark.parametrize("unique", [True, False])
+def test_join_compact_fingerprint_collisions(dtype, unique):
+    # a 2^7-bucket COMPACT table compares 7 bucket + 16 fingerprint hash
+    # bits: probe keys built to agree with a build key on those 23 bits but
+    # not on the key must be rejected by the full-key check, and the walk
+    # must go on to the true match when there is one
+    a, b = _fingerprint_twins(dtype, 3000)
+    build = np.concatenate([a, b[:1000]])           # some twins are both present
+    if not unique:
+        build = np.concatenate([build, a[:500]])
+    probe = np.concatenate([b, a, b[:1000]])
+    rng = np.random.default_rng(23)
+    rng.shuffle(build)
+    rng.shuffle(probe)
+    plan = api.plan_default(build.shape[0], probe.shape[0], np.dtype(dtype).itemsize, unique)
+    plan.table_mode, plan.digit_mode, plan.bits1 = TABLE_COMPACT, DIGIT_RAW, 0
+    plan.split_mode = SPLIT_POSITION
+    plan.table_capacity = 256                      # 2^7 buckets
+    br, pr = run(build, probe, unique, plan)
+    assert pairs_equal(build, probe, br, pr, unique)
+
+
+def test_join_compact_default_plan_large_partitions():
+    # past one pass's fan-out the default plan takes COMPACT tables
+    b, p = datagen.config2(seed=22, n_build=1 << 22, n_probe=1 << 22)
+    plan = api.plan_default(b.shape[0], p.shape[0], 4)
+    plan.table_mode = TABLE_COMPACT
+    plan.table_capacity = 41472 // 128 * 128
+    plan.bits1 = 7                 # 32 K build tuples per partition, no split
     br, pr = run(b, p, True, plan)
     assert pairs_equal(b, p, br, pr)
 
