@@ -223,7 +223,7 @@ def run_ours(args, rank, world, local):
     import torch
     import torch.distributed as dist
 
-    from partitioned_join_b200 import _lib, api
+    from partitioned_join_b200 import _lib, api, replicas
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
@@ -232,7 +232,8 @@ def run_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
 
     n_b, n_p = 1 << args.log2_build, 1 << args.log2_probe
-    build, probe, expected = gen_config2_device(n_b, n_p, args.match_rate, args.seed + rank, device)
+    build, probe, expected = gen_config2_device(n_b, n_p, args.match_rate, replicas.replica_seed(args.seed, rank),
+                                                device)
     # the exact-histogram planner picks the digit source (and split) from the data
     plan = api.plan_exact(build, probe, True) if not args.default_plan else api.plan_default(n_b, n_p, 4, True)
     if args.plan:
@@ -261,30 +262,24 @@ def run_ours(args, rank, world, local):
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
     clocks.start()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     t0.record(stream)
     for k in range(args.steps):
         j.launch_with_events(ev[k])
     t1.record(stream)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     clk = clocks.stop()
     _lib.check(j.status(), "timed joins")
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        t = torch.tensor([ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(t0.elapsed_time(t1), device)
     stage_ms = {name: 0.0 for name in _lib.STAGES[:-1]}
     for row in ev:
         for i, name in enumerate(_lib.STAGES[:-1]):
             stage_ms[name] += row[i].elapsed_time(row[i + 1]) / args.steps
     step_ms = ms / args.steps
-    tuples_all = world * (n_b + n_p) * args.steps
-    value = tuples_all / (ms / 1e3)
+    tuples_all = replicas.sum_over_ranks((n_b + n_p) * args.steps, device)
+    value = replicas.whole_job_rate(tuples_all, ms)
 
     # roofline: the dominant kernel and the whole join
     peak, peak_kind = measured_peak_gbs()

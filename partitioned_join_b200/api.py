@@ -45,7 +45,11 @@ def _keys(t: torch.Tensor, name: str) -> torch.Tensor:
     return t
 
 
-def make_desc(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_keys: bool = True) -> JoinDesc:
+PAYLOAD_DTYPES = {torch.int32: 4, torch.int64: 8, torch.float32: 4, torch.float64: 8}
+
+
+def make_desc(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_keys: bool = True,
+              build_payload: Optional[torch.Tensor] = None, probe_payload: Optional[torch.Tensor] = None) -> JoinDesc:
     b = _keys(build_keys, "build_keys")
     p = _keys(probe_keys, "probe_keys")
     if b.dtype != p.dtype:
@@ -58,6 +62,20 @@ def make_desc(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_k
     d.key_bytes = KEY_DTYPES[b.dtype]
     d.payload_bytes = 0
     d.unique_build_keys = 1 if unique_build_keys else 0
+    pays = [(t, n, side) for t, n, side in ((build_payload, b.numel(), "build"), (probe_payload, p.numel(), "probe"))
+            if t is not None]
+    for t, n, side in pays:
+        if not t.is_cuda or t.dim() != 1 or t.numel() != n or t.dtype not in PAYLOAD_DTYPES or not t.is_contiguous():
+            raise ValueError(f"{side}_payload must be a contiguous CUDA column of 4- or 8-byte values, one per key")
+    if pays:
+        widths = {PAYLOAD_DTYPES[t.dtype] for t, _, _ in pays}
+        if len(widths) != 1:
+            raise ValueError("build and probe payloads must have the same width")
+        d.payload_bytes = widths.pop()
+        if build_payload is not None:
+            d.build_payload = build_payload.data_ptr()
+        if probe_payload is not None:
+            d.probe_payload = probe_payload.data_ptr()
     return d
 
 
@@ -181,6 +199,31 @@ def partitioned_join(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_
         j = Joiner(build_keys, probe_keys, unique_build_keys, j.plan, n)
         j.launch(stream)
     return j.result(stream)
+
+
+def partitioned_join_payload(build_keys: torch.Tensor, probe_keys: torch.Tensor,
+                             build_payload: Optional[torch.Tensor], probe_payload: Optional[torch.Tensor],
+                             unique_build_keys: bool = True, plan: Optional[Plan] = None, stream=None):
+    """The join plus payload materialisation: (build_row, probe_row,
+    build_payload[build_row], probe_payload[probe_row]) -- the reference's
+    joined {key, probe_val} records (hash_join_kernels.cuh:155-163) as
+    columns.  A payload argument may be None (its output is then None)."""
+    b = _keys(build_keys, "build_keys")
+    p = _keys(probe_keys, "probe_keys")
+    desc = make_desc(b, p, unique_build_keys, build_payload, probe_payload)
+    j = Joiner(b, p, unique_build_keys, plan)  # output sized by pj_join_count for repeated keys
+    dev = b.device
+    pb = torch.empty(max(j.capacity, 1), dtype=build_payload.dtype, device=dev) if build_payload is not None else None
+    pp = torch.empty(max(j.capacity, 1), dtype=probe_payload.dtype, device=dev) if probe_payload is not None else None
+    out = j._out()
+    out.build_payload_out = pb.data_ptr() if pb is not None else None
+    out.probe_payload_out = pp.data_ptr() if pp is not None else None
+    check(lib().pj_inner_join(ctypes.byref(desc), ctypes.byref(j.plan), ctypes.byref(out),
+                              ctypes.c_void_p(j.ws.data_ptr()), j.ws_bytes, _stream_ptr(stream)), "pj_inner_join")
+    check(j.status(stream), "pj_inner_join")
+    n = int(j.count.item())
+    return (j.build_row[:n], j.probe_row[:n], pb[:n] if pb is not None else None,
+            pp[:n] if pp is not None else None)
 
 
 def inner_join_noalloc(build_keys: torch.Tensor, probe_keys: torch.Tensor, capacity: int,

@@ -331,6 +331,24 @@ __global__ void hash_slots_kernel(const K* __restrict__ keys, int64_t n, int32_t
     }
 }
 
+// Payload materialisation after the join: dst[i] = src[row[i]] for the
+// count entries written (the step after the join in a query engine; the
+// reference emits the probe payload inside its join record instead,
+// hash_join_kernels.cuh:155-163).  Either side may be absent.
+template <typename T>
+__global__ void gather_payload_kernel(const int32_t* __restrict__ build_row, const int32_t* __restrict__ probe_row,
+                                      const T* __restrict__ build_src, const T* __restrict__ probe_src,
+                                      T* __restrict__ build_dst, T* __restrict__ probe_dst,
+                                      const unsigned long long* __restrict__ count, int64_t capacity)
+{
+    const long long n = static_cast<long long>(*count) < capacity ? static_cast<long long>(*count) : capacity;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        if (build_dst) build_dst[i] = build_src[build_row[i]];
+        if (probe_dst) probe_dst[i] = probe_src[probe_row[i]];
+    }
+}
+
 // Partition boundaries from the flattened segment offsets: part[p] = off[p*items].
 __global__ void partition_bounds_kernel(const int64_t* __restrict__ off, int32_t items, int32_t P,
                                         int64_t* __restrict__ part)
@@ -494,7 +512,7 @@ pj_status partition_column(const K* keys, int64_t n, const pj_plan* p, const Lay
 
 template <typename K>
 pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uint8_t* ws, int32_t* out_b,
-                   int32_t* out_p, int64_t capacity, int64_t* count, cudaStream_t st,
+                   int32_t* out_p, int64_t capacity, int64_t* count, void* pay_b, void* pay_p, cudaStream_t st,
                    const StageEvents& E = StageEvents())
 {
     uint32_t* status = reinterpret_cast<uint32_t*>(ws + L.status);
@@ -565,6 +583,19 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     a.max_ctas = L.max_ctas;
     E.mark(PJ_STAGE_JOIN, st);
     s = launch_join<K>(a, p->table_mode, d->unique_build_keys != 0, hash_split, p->slot_mode == PJ_SLOT_REF, st);
+    if (s == PJ_OK && out_b && (pay_b || pay_p) && d->payload_bytes > 0) {
+        const unsigned grid = static_cast<unsigned>(sm_count()) * 8;
+        const auto* cnt = reinterpret_cast<const unsigned long long*>(count);
+        if (d->payload_bytes == 4)
+            gather_payload_kernel<int32_t><<<grid, 256, 0, st>>>(
+                out_b, out_p, static_cast<const int32_t*>(d->build_payload), static_cast<const int32_t*>(d->probe_payload),
+                static_cast<int32_t*>(pay_b), static_cast<int32_t*>(pay_p), cnt, capacity);
+        else
+            gather_payload_kernel<int64_t><<<grid, 256, 0, st>>>(
+                out_b, out_p, static_cast<const int64_t*>(d->build_payload), static_cast<const int64_t*>(d->probe_payload),
+                static_cast<int64_t*>(pay_b), static_cast<int64_t*>(pay_p), cnt, capacity);
+        PJ_CUDA(cudaGetLastError());
+    }
     E.mark(PJ_STAGE_TOTAL, st);
     return s;
 }
@@ -593,10 +624,15 @@ pj_status check_inputs(const pj_join_desc* d)
     return PJ_OK;
 }
 
-pj_status check_output(const pj_output* out)
+pj_status check_output(const pj_join_desc* d, const pj_output* out)
 {
     if (!out || !out->count || out->capacity < 0) return PJ_ERR_INVALID;
     if (out->capacity > 0 && (!out->build_row || !out->probe_row)) return PJ_ERR_INVALID;
+    // a payload output needs its payload column
+    if (d && d->payload_bytes > 0) {
+        if (out->build_payload_out && d->n_build > 0 && !d->build_payload) return PJ_ERR_INVALID;
+        if (out->probe_payload_out && d->n_probe > 0 && !d->probe_payload) return PJ_ERR_INVALID;
+    }
     return PJ_OK;
 }
 
@@ -609,12 +645,17 @@ pj_status prepare(const pj_join_desc* d, const pj_plan* plan, void* ws, size_t w
     return check_ws(d, p, ws, ws_bytes, L);
 }
 
-pj_status dispatch_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, void* ws, int32_t* ob, int32_t* op,
-                        int64_t cap, int64_t* count, cudaStream_t st, const StageEvents& E)
+pj_status dispatch_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, void* ws, const pj_output* out,
+                        int64_t* count, cudaStream_t st, const StageEvents& E)
 {
     uint8_t* w = static_cast<uint8_t*>(ws);
-    if (d->key_bytes == 4) return run_join<int32_t>(d, p, L, w, ob, op, cap, count, st, E);
-    return run_join<int64_t>(d, p, L, w, ob, op, cap, count, st, E);
+    int32_t* ob = out ? out->build_row : nullptr;
+    int32_t* op = out ? out->probe_row : nullptr;
+    const int64_t cap = out ? out->capacity : 0;
+    void* pb = out ? out->build_payload_out : nullptr;
+    void* pp = out ? out->probe_payload_out : nullptr;
+    if (d->key_bytes == 4) return run_join<int32_t>(d, p, L, w, ob, op, cap, count, pb, pp, st, E);
+    return run_join<int64_t>(d, p, L, w, ob, op, cap, count, pb, pp, st, E);
 }
 
 }  // namespace
@@ -699,19 +740,19 @@ pj_status pj_workspace_size(const pj_join_desc* d, const pj_plan* plan, size_t* 
 pj_status pj_inner_join(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws, size_t ws_bytes,
                         pj_stream stream)
 {
-    pj_status s = check_output(out);
+    pj_status s = check_output(d, out);
     if (s != PJ_OK) return s;
     pj_plan p;
     Layout L;
     if ((s = prepare(d, plan, ws, ws_bytes, &p, &L)) != PJ_OK) return s;
-    return dispatch_join(d, &p, L, ws, out->build_row, out->probe_row, out->capacity, out->count,
+    return dispatch_join(d, &p, L, ws, out, out->count,
                          static_cast<cudaStream_t>(stream), StageEvents());
 }
 
 pj_status pj_inner_join_events(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws,
                                size_t ws_bytes, pj_stream stream, void* const* events)
 {
-    pj_status s = check_output(out);
+    pj_status s = check_output(d, out);
     if (s != PJ_OK) return s;
     if (!events) return PJ_ERR_INVALID;
     for (int i = 0; i < PJ_NUM_STAGES; ++i)
@@ -721,14 +762,14 @@ pj_status pj_inner_join_events(const pj_join_desc* d, const pj_plan* plan, pj_ou
     if ((s = prepare(d, plan, ws, ws_bytes, &p, &L)) != PJ_OK) return s;
     StageEvents E;
     E.ev = reinterpret_cast<cudaEvent_t*>(const_cast<void**>(events));
-    return dispatch_join(d, &p, L, ws, out->build_row, out->probe_row, out->capacity, out->count,
+    return dispatch_join(d, &p, L, ws, out, out->count,
                          static_cast<cudaStream_t>(stream), E);
 }
 
 pj_status pj_inner_join_timed(const pj_join_desc* d, const pj_plan* plan, pj_output* out, void* ws,
                               size_t ws_bytes, pj_stream stream, float* stage_ms)
 {
-    pj_status s = check_output(out);
+    pj_status s = check_output(d, out);
     if (s != PJ_OK) return s;
     if (!stage_ms) return PJ_ERR_INVALID;
     pj_plan p;
@@ -739,7 +780,7 @@ pj_status pj_inner_join_timed(const pj_join_desc* d, const pj_plan* plan, pj_out
     for (int i = 0; i < PJ_NUM_STAGES; ++i) PJ_CUDA(cudaEventCreate(&ev[i]));
     StageEvents E;
     E.ev = ev;
-    s = dispatch_join(d, &p, L, ws, out->build_row, out->probe_row, out->capacity, out->count, st, E);
+    s = dispatch_join(d, &p, L, ws, out, out->count, st, E);
     cudaError_t e = cudaStreamSynchronize(st);
     if (s == PJ_OK && e == cudaSuccess) {
         for (int i = 0; i + 1 < PJ_NUM_STAGES; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
@@ -762,7 +803,7 @@ pj_status pj_join_count(const pj_join_desc* d, const pj_plan* plan, int64_t* cou
     pj_status s = prepare(d, plan, ws, ws_bytes, &p, &L);
     if (s != PJ_OK) return s;
     // no output columns: the join counts every match and writes none
-    return dispatch_join(d, &p, L, ws, nullptr, nullptr, 0, count_dev, static_cast<cudaStream_t>(stream),
+    return dispatch_join(d, &p, L, ws, nullptr, count_dev, static_cast<cudaStream_t>(stream),
                          StageEvents());
 }
 

@@ -292,6 +292,26 @@ def test_capacity_error_reports_required_count():
     assert "capacity" in str(e.value)
 
 
+@pytest.mark.parametrize("pdtype", [np.int32, np.int64, np.float32])
+@pytest.mark.parametrize("unique", [True, False])
+def test_join_payload_gather(pdtype, unique):
+    rng = np.random.default_rng(24)
+    b = rng.permutation(300000).astype(np.int32)
+    if not unique:
+        b = np.concatenate([b, b[:20000]])
+    p = rng.integers(0, 400000, size=500000).astype(np.int32)
+    bp = (rng.standard_normal(b.shape[0]) * 1000).astype(pdtype)
+    pp = (rng.standard_normal(p.shape[0]) * 1000).astype(pdtype)
+    br, pr, gb, gp = api.partitioned_join_payload(dev(b), dev(p), dev(bp), dev(pp), unique_build_keys=unique)
+    br, pr = br.cpu().numpy(), pr.cpu().numpy()
+    assert np.array_equal(gb.cpu().numpy(), bp[br])
+    assert np.array_equal(gp.cpu().numpy(), pp[pr])
+    assert pairs_equal(b, p, torch.from_numpy(br), torch.from_numpy(pr), unique)
+    # one side only
+    _, pr2, none_b, gp2 = api.partitioned_join_payload(dev(b), dev(p), None, dev(pp), unique_build_keys=unique)
+    assert none_b is None and np.array_equal(gp2.cpu().numpy(), pp[pr2.cpu().numpy()])
+
+
 def test_join_count_matches_oracle():
     b, p = datagen.config2(seed=17, n_build=100000, n_probe=200000)
     assert api.join_count(dev(b), dev(p)) == oracle.inner_join(b, p)[0].shape[0]
