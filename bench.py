@@ -70,20 +70,13 @@ def dist_env():
 # inputs
 
 def gen_config2_device(n_b, n_p, match_rate, seed, device):
-    """Seeded cfg2-shaped inputs generated on the device (torch RNG)."""
+    """Seeded cfg2-shaped inputs generated on the device by the library's
+    own generator (pj_generate_tables): build = a seeded permutation of
+    0..n_b-1, probe = a uniform build key with probability match_rate, else a
+    key above n_b-1.  Returns (build, probe, matching probe rows)."""
     import torch
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    build = (torch.randperm(n_b, generator=g, device=device) + 1).to(torch.int32)
-    idx = torch.randint(0, n_b, (n_p,), generator=g, device=device)
-    probe = build[idx]
-    del idx
-    miss = torch.rand(n_p, generator=g, device=device) >= match_rate
-    nm = int(miss.sum().item())
-    if nm:
-        probe[miss] = torch.randint(n_b + 1, 2**31 - 1, (nm,), generator=g, device=device).to(torch.int32)
-    expected = int((probe <= n_b).sum().item())
-    return build.contiguous(), probe.contiguous(), expected
+    from partitioned_join_b200 import api
+    return api.generate_tables(n_b, n_p, torch.int32, n_b - 1, match_rate, True, 0.0, seed, device)
 
 
 def cpu_sample(log2n, match_rate, seed):
@@ -304,7 +297,8 @@ def run_ours(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2): build = seeded "
-                               f"permutation of 1..2^{args.log2_build}, probe {args.match_rate:.0%} uniform hits",
+                               f"permutation of 0..2^{args.log2_build}-1, probe {args.match_rate:.0%} uniform hits, "
+                               f"the rest above the build keys (generated on the device)",
                    "build_rows": n_b, "probe_rows": n_p, "output_pairs": expected, "unique_build_keys": True,
                    "l2": "inputs (1 GiB) larger than L2, no flush", "parallelism": f"replicas x{world}",
                    "plan": plan.as_dict()},

@@ -253,6 +253,21 @@ pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_
                        void* tuples, int64_t* offsets, void* workspace, size_t workspace_bytes,
                        pj_stream stream);
 
+/* Seeded input tables generated on the device: the reference's
+ * generate_input_tables (generate_input_tables.cuh:143-226) and its Zipf
+ * generator (generate_zipf_input.cuh:50-134).  Build keys lie in
+ * [0, rand_max] (distinct when unique_build_keys, which needs
+ * rand_max + 1 >= n_build); each probe key is a build key with probability
+ * selectivity -- uniformly chosen, or by a Zipf(zipf_theta) law over a
+ * seeded rank order when zipf_theta > 0 -- and otherwise a value no build
+ * row holds (for repeated build keys: a value above rand_max).  Every value
+ * is a pure function of (seed, row).  *hits_dev (device int64, optional)
+ * receives the number of probe rows drawn from the build side.
+ * Asynchronous. */
+pj_status pj_generate_tables(void* build_keys, int64_t n_build, void* probe_keys, int64_t n_probe,
+                             int32_t key_bytes, int64_t rand_max, double selectivity, int32_t unique_build_keys,
+                             double zipf_theta, uint64_t seed, int64_t* hits_dev, pj_stream stream);
+
 /* Capacity in tuples that pj_partition needs for n keys under plan. */
 pj_status pj_partitioned_capacity(int64_t n, int32_t key_bytes, const pj_plan* plan,
                                   int64_t* tuples);

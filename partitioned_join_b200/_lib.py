@@ -68,6 +68,8 @@ SIGNATURES = {
     "pj_radix_histogram": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "pj_partition": (ctypes.c_int, [_P, _I64, _I32, ctypes.POINTER(Plan), _P, _P, _P, _SZ, _P]),
     "pj_partitioned_capacity": (ctypes.c_int, [_I64, _I32, ctypes.POINTER(Plan), ctypes.POINTER(_I64)]),
+    "pj_generate_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I64, ctypes.c_double, _I32, ctypes.c_double,
+                                          ctypes.c_uint64, _P, _P]),
 }
 
 _lib = None

@@ -226,6 +226,27 @@ def partitioned_join_payload(build_keys: torch.Tensor, probe_keys: torch.Tensor,
             pp[:n] if pp is not None else None)
 
 
+def generate_tables(n_build: int, n_probe: int, key_dtype=torch.int32, rand_max: Optional[int] = None,
+                    selectivity: float = 1.0, unique_build_keys: bool = True, zipf_theta: float = 0.0,
+                    seed: int = 1, device="cuda", stream=None):
+    """Seeded input tables generated on the device (pj_generate_tables): the
+    reference's generate_input_tables recipe plus Zipf-distributed probe
+    hits.  rand_max defaults to n_build - 1 (unique keys: a permutation of
+    0..n_build-1).  Returns (build_keys, probe_keys, hits), hits = probe rows
+    drawn from the build side."""
+    kb = KEY_DTYPES[key_dtype]
+    if rand_max is None:
+        rand_max = max(n_build - 1, 0)
+    b = torch.empty(max(n_build, 1), dtype=key_dtype, device=device)[:n_build]
+    p = torch.empty(max(n_probe, 1), dtype=key_dtype, device=device)[:n_probe]
+    hits = torch.zeros(1, dtype=torch.int64, device=device)
+    check(lib().pj_generate_tables(ctypes.c_void_p(b.data_ptr()), n_build, ctypes.c_void_p(p.data_ptr()), n_probe, kb,
+                                   rand_max, float(selectivity), 1 if unique_build_keys else 0, float(zipf_theta),
+                                   seed & (2**64 - 1), ctypes.c_void_p(hits.data_ptr()), _stream_ptr(stream)),
+          "pj_generate_tables")
+    return b, p, int(hits.item())
+
+
 def inner_join_noalloc(build_keys: torch.Tensor, probe_keys: torch.Tensor, capacity: int,
                        unique_build_keys: bool = True, plan: Optional[Plan] = None,
                        stream=None) -> Tuple[torch.Tensor, torch.Tensor]:

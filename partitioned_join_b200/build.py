@@ -21,11 +21,14 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["pj_api.cu", "pj_noalloc.cu"]
+LIB_SOURCES = ["pj_api.cu", "pj_noalloc.cu", "pj_generate.cu"]
 
 
 def _deps():
     files = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h", ".cpp"))]
+    cli_dir = os.path.join(CSRC, "cli")
+    if os.path.isdir(cli_dir):
+        files += [os.path.join(cli_dir, f) for f in os.listdir(cli_dir)]
     files.append(os.path.join(ROOT, "include", "pj.h"))
     return files
 
@@ -45,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> None:
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)
-    cli_src = os.path.join(CSRC, "cli", "partitioned_join_cli.cpp")
+    cli_src = os.path.join(CSRC, "cli", "partitioned_join_cli.cu")
     if os.path.exists(cli_src) and (force or _stale(CLI, deps + [cli_src, LIB])):
         os.makedirs(BIN_DIR, exist_ok=True)
         cmd = [NVCC, *COMMON, cli_src, "-o", CLI, "-L", PKG, "-lpj", "-Xlinker", "-rpath,$ORIGIN/..",
