@@ -46,8 +46,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--log2-build", type=int, default=27)
-    ap.add_argument("--log2-probe", type=int, default=27)
+    ap.add_argument("--workload", choices=["cfg2", "cfg3"], default="cfg2",
+                    help="cfg2: 2^27 x 2^27 int32 uniform (the headline); cfg3: 2^26 x 2^28 int64, Zipf probe keys")
+    ap.add_argument("--zipf", type=float, default=1.0, help="cfg3: Zipf exponent of the probe keys")
+    ap.add_argument("--log2-build", type=int, default=None)
+    ap.add_argument("--log2-probe", type=int, default=None)
     ap.add_argument("--match-rate", type=float, default=0.9)
     ap.add_argument("--cpu-sample-log2", type=int, default=24,
                     help="build and probe rows of the bounded CPU sample (log2)")
@@ -56,7 +59,12 @@ def parse_args():
     ap.add_argument("--plan", type=str, default="", help="JSON overrides of pj_plan fields")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--default-plan", action="store_true", help="plan from sizes only (no histogram)")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.log2_build is None:
+        a.log2_build = 27 if a.workload == "cfg2" else 26
+    if a.log2_probe is None:
+        a.log2_probe = 27 if a.workload == "cfg2" else 28
+    return a
 
 
 def dist_env():
@@ -225,10 +233,16 @@ def run_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
 
     n_b, n_p = 1 << args.log2_build, 1 << args.log2_probe
-    build, probe, expected = gen_config2_device(n_b, n_p, args.match_rate, replicas.replica_seed(args.seed, rank),
-                                                device)
+    seed = replicas.replica_seed(args.seed, rank)
+    if args.workload == "cfg2":
+        build, probe, expected = gen_config2_device(n_b, n_p, args.match_rate, seed, device)
+    else:
+        # unique random int64 build keys, every probe key a build key drawn by Zipf(args.zipf)
+        build, probe, expected = api.generate_tables(n_b, n_p, torch.int64, (1 << 62) - 1, 1.0, True, args.zipf, seed,
+                                                     device)
+    kb = build.element_size()
     # the exact-histogram planner picks the digit source (and split) from the data
-    plan = api.plan_exact(build, probe, True) if not args.default_plan else api.plan_default(n_b, n_p, 4, True)
+    plan = api.plan_exact(build, probe, True) if not args.default_plan else api.plan_default(n_b, n_p, kb, True)
     if args.plan:
         for k, v in json.loads(args.plan).items():
             setattr(plan, k, v)
@@ -276,7 +290,7 @@ def run_ours(args, rank, world, local):
 
     # roofline: the dominant kernel and the whole join
     peak, peak_kind = measured_peak_gbs()
-    kb, tb = 4, 8  # key bytes, partitioned tuple bytes
+    tb = 8 if kb == 4 else 12  # partitioned tuple bytes
     alg = {
         "build_hist": n_b * kb, "probe_hist": n_p * kb,
         "build_scatter": n_b * (kb + tb), "probe_scatter": n_p * (kb + tb),
@@ -288,17 +302,21 @@ def run_ours(args, rank, world, local):
                  "build_scatter": "scatter_keys_kernel", "probe_scatter": "scatter_keys_kernel",
                  "join": "join_kernel"}
     traffic = ncu_traffic(f"{kernel_of[dom]}:{dom}")
-    b_alg = (n_b + n_p) * (4 + 4) + expected * 8          # (k+v) per input tuple + 8 per output pair
-    b_keys = (n_b + n_p) * 4 + expected * 8               # what the path must move at least
+    b_alg = (n_b + n_p) * (kb + kb) + expected * 8        # (k+v) per input tuple + 8 per output pair
+    b_keys = (n_b + n_p) * kb + expected * 8              # what the path must move at least
     join_gbs = b_alg / (step_ms / 1e3) / 1e9
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC if args.workload == "cfg2" else "tuples/s, 2^26x2^28 int64 Zipf join",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2): build = seeded "
-                               f"permutation of 0..2^{args.log2_build}-1, probe {args.match_rate:.0%} uniform hits, "
-                               f"the rest above the build keys (generated on the device)",
+        "vs_baseline": None, "dtype": "int32" if kb == 4 else "int64", "data": "synthetic",
+        "config": {"workload": (f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2): build = seeded "
+                                f"permutation of 0..2^{args.log2_build}-1, probe {args.match_rate:.0%} uniform hits, "
+                                f"the rest above the build keys (generated on the device)")
+                   if args.workload == "cfg2" else
+                   (f"2^{args.log2_build}x2^{args.log2_probe} int64 inner join (cfg3): unique random build keys, "
+                    f"probe keys Zipf({args.zipf}) over a seeded rank order (generated on the device)"),
                    "build_rows": n_b, "probe_rows": n_p, "output_pairs": expected, "unique_build_keys": True,
                    "l2": "inputs (1 GiB) larger than L2, no flush", "parallelism": f"replicas x{world}",
                    "plan": plan.as_dict()},
@@ -334,7 +352,7 @@ def e2e_measure(args, j, build, probe, stream):
     op = torch.empty(cap, dtype=torch.int32).pin_memory()
     cnt = torch.empty(1, dtype=torch.int64).pin_memory()
     steps = max(1, min(args.steps, 5))
-    h2d = hb.numel() * 4 + hp.numel() * 4
+    h2d = hb.numel() * hb.element_size() + hp.numel() * hp.element_size()
     d2h = []
 
     def step():

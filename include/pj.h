@@ -108,6 +108,9 @@ enum {
                              a build range must stay within 65536 tuples */
 };
 
+/* Most heavy probe keys a plan can name. */
+#define PJ_MAX_HEAVY 256
+
 /* Execution plan.  pj_plan_default() fills it from the sizes alone,
  * pj_plan_exact() from device histograms.  Passing NULL to pj_inner_join()
  * uses pj_plan_default(). */
@@ -126,6 +129,12 @@ typedef struct pj_plan {
     int32_t hist_split;         /* histogram CTAs per scatter chunk */
     float max_fill;             /* OPEN: target fill (the reference's HASH_TABLE_OCC = 0.5) */
     int32_t flags;              /* reserved, 0 */
+    int32_t n_heavy;            /* heavy probe keys below (0: no heavy-key path) */
+    int32_t heavy_reserved;     /* 0 */
+    int64_t heavy_keys[PJ_MAX_HEAVY]; /* probe keys matched outside the partitions, by a
+                                   table every CTA holds (unique build keys only);
+                                   the reference's skewed_data_handler.cuh:21-91 instead
+                                   splits the oversized partitions they cause */
 } pj_plan;
 
 /* Human-readable text of a status. */
@@ -245,8 +254,9 @@ pj_status pj_radix_histogram(const void* keys, int64_t n, int32_t key_bytes, int
 /* Radix-partitions one key column into `tuples` (device, capacity
  * pj_partitioned_capacity() tuples) with partition p occupying tuples
  * [offsets[p], offsets[p+1]) (offsets: device int64, 2^(bits1+bits2)+1).
- * A tuple is {int32 key, int32 row} for 4-byte keys and {int32 key_lo,
- * int32 key_hi, int32 row} for 8-byte keys; padding tuples carry row = -1.
+ * A tuple is {uint32 murmur(key), int32 row} for 4-byte keys (the hash is a
+ * bijection of the key) and {int32 key_lo, int32 key_hi, uint32 murmur(key),
+ * int32 row} for 8-byte keys; padding tuples carry row = -1.
  * Replaces partition_input_tables_pass_one / _pass_two
  * (partitioned_join.cuh:51-175). */
 pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_plan* plan,

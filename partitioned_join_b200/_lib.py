@@ -15,6 +15,7 @@ SLOT_FAST, SLOT_REF = 0, 1
 SPLIT_HASH, SPLIT_POSITION = 0, 1
 TABLE_BUCKET, TABLE_OPEN, TABLE_COMPACT = 0, 1, 2
 NOALLOC_SCRATCH_BYTES = 64 << 20  # PJ_NOALLOC_SCRATCH_BYTES
+MAX_HEAVY = 256                   # PJ_MAX_HEAVY
 STAGES = ["build_hist", "build_scan", "build_scatter", "probe_hist", "probe_scan", "probe_scatter", "join_plan",
           "join", "total"]
 
@@ -38,10 +39,19 @@ class Plan(ctypes.Structure):
                 ("digit_mode", ctypes.c_int32), ("table_mode", ctypes.c_int32), ("slot_mode", ctypes.c_int32),
                 ("split_mode", ctypes.c_int32), ("table_capacity", ctypes.c_int32), ("probe_chunk", ctypes.c_int32),
                 ("wc_tuples", ctypes.c_int32), ("scatter_ctas_per_sm", ctypes.c_int32), ("hist_split", ctypes.c_int32),
-                ("max_fill", ctypes.c_float), ("flags", ctypes.c_int32)]
+                ("max_fill", ctypes.c_float), ("flags", ctypes.c_int32), ("n_heavy", ctypes.c_int32),
+                ("heavy_reserved", ctypes.c_int32), ("heavy_keys", ctypes.c_int64 * MAX_HEAVY)]
 
     def as_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "heavy_keys"}
+        d["heavy_keys"] = list(self.heavy_keys[: max(0, min(self.n_heavy, MAX_HEAVY))])
+        return d
+
+    def set_heavy(self, keys):
+        keys = list(keys)[:MAX_HEAVY]
+        self.n_heavy = len(keys)
+        for i, k in enumerate(keys):
+            self.heavy_keys[i] = int(k)
 
     def __repr__(self):
         return "Plan(" + ", ".join(f"{k}={v}" for k, v in self.as_dict().items()) + ")"

@@ -330,7 +330,7 @@ def partition(keys: torch.Tensor, plan: Plan) -> Tuple[torch.Tensor, torch.Tenso
     kb = KEY_DTYPES[k.dtype]
     cap = ctypes.c_int64(0)
     check(lib().pj_partitioned_capacity(k.numel(), kb, ctypes.byref(plan), ctypes.byref(cap)), "pj_partitioned_capacity")
-    words = 2 if kb == 4 else 3
+    words = 2 if kb == 4 else 4
     tuples = torch.empty(cap.value * words + 16, dtype=torch.int32, device=k.device)
     P = 1 << (plan.bits1 + (plan.bits2 if plan.passes == 2 else 0))
     offsets = torch.empty(P + 1, dtype=torch.int64, device=k.device)

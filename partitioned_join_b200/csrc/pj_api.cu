@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -14,6 +16,7 @@
 #include "pj_partition.cuh"
 
 using namespace pj;
+static_assert(MAX_HEAVY == PJ_MAX_HEAVY, "heavy-key capacity of the plan");
 
 namespace {
 
@@ -29,6 +32,10 @@ constexpr int JN_THREADS = PJ_JOIN_THREADS;
 constexpr int MAX_SPLIT_LOG2 = 6;
 constexpr int MAX_BUCKET_CAP = 65535;  // 16-bit bucket ends
 constexpr int MAX_JOIN_CTAS_PER_SM = 4;
+constexpr int HEAVY_SAMPLES = 1 << 16;     // probe keys the planner samples
+constexpr int HEAVY_MIN_SAMPLES = 32;      // a heavy key holds >= 1/2048 of the sample
+constexpr int64_t HEAVY_MIN_PROBE = 1 << 20;  // smaller probe sides: no heavy-key path
+constexpr double HEAVY_MIN_SHARE = 0.5;       // share of the probe rows the heavy keys must hold
 
 struct DevInfo {
     int device = -1;
@@ -92,7 +99,7 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 template <typename K>
 constexpr int sc_v() { return sizeof(K) == 4 ? SC_V32 : SC_V64; }
 
-int tuple_words(int key_bytes) { return key_bytes == 4 ? 2 : 3; }
+int tuple_words(int key_bytes) { return key_bytes == 4 ? 2 : 4; }
 
 size_t scatter_smem(int key_bytes, int W, int P)
 {
@@ -170,6 +177,9 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (p->scatter_ctas_per_sm < 1 || p->scatter_ctas_per_sm > 8) return PJ_ERR_INVALID;
     if (p->hist_split < 1 || p->hist_split > 16) return PJ_ERR_INVALID;
     if (p->table_mode == PJ_TABLE_OPEN && !(p->max_fill > 0.05f && p->max_fill <= 0.95f)) return PJ_ERR_INVALID;
+    if (p->n_heavy < 0 || p->n_heavy > PJ_MAX_HEAVY) return PJ_ERR_INVALID;
+    if (p->n_heavy > 0 && scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) + HeavyTable::BYTES + 16 > smem_limit())
+        return PJ_ERR_INVALID;  // the probe scatter also holds the heavy table
     // hash bits: digits + hash split + bucket/slot bits must fit 32
     const int digit_bits = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0;
     const int slot_bits = p->table_mode != PJ_TABLE_OPEN ? bucket_nb_log2(p->table_capacity) : 12;
@@ -202,7 +212,8 @@ struct Layout {
     int64_t b_cap = 0, p_cap = 0;  // tuples
     int64_t max_items = 0;
     size_t status = 0, counters = 0, b_tiles = 0, p_tiles = 0, i_tiles = 0, b_tot = 0, p_tot = 0;
-    size_t b_counts = 0, p_counts = 0, ctrl_end = 0;
+    size_t b_counts = 0, p_counts = 0, heavy_total = 0, heavy_items = 0, ctrl_end = 0;
+    size_t heavy_row = 0, sample = 0;
     size_t b_off = 0, p_off = 0, split = 0, items = 0, item_off = 0, item_part = 0;
     size_t cta_q = 0, cta_last = 0, seg = 0, over_b = 0, over_p = 0;
     int max_ctas = 0;
@@ -256,7 +267,11 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.p_tot = take(4 * static_cast<size_t>(L.P));
     L.b_counts = take(4 * static_cast<size_t>(mb));
     L.p_counts = take(4 * static_cast<size_t>(mp));
+    L.heavy_total = take(8);
+    L.heavy_items = take(8 * static_cast<size_t>(L.p_items));
     L.ctrl_end = o;
+    L.heavy_row = take(4 * MAX_HEAVY);
+    L.sample = take(8 * static_cast<size_t>(HEAVY_SAMPLES));
     L.b_off = take(8 * static_cast<size_t>(mb + 1));
     L.p_off = take(8 * static_cast<size_t>(mp + 1));
     L.split = take(4 * static_cast<size_t>(L.P));
@@ -366,22 +381,37 @@ unsigned grid_for(int64_t n, int threads)
 // ---------------------------------------------------------------------------
 // Stage launchers.
 
-template <typename K>
-pj_status launch_hist(const K* keys, int64_t n, int64_t chunk, int items, int hsplit, DigitFn f, int P,
-                      uint32_t* counts, int32_t* totals, cudaStream_t st)
+// Heavy probe keys of one join: the set and where their pairs go.
+struct HeavyCtx {
+    const HeavySet* hs = nullptr;  // nullptr: no heavy path
+    HeavyOut out{};
+};
+
+template <typename K, bool HASHD, bool HEAVY>
+pj_status launch_hist_t(const K* keys, int64_t n, int64_t chunk, int items, int hsplit, DigitFn f, int P,
+                        uint32_t* counts, int32_t* totals, const HeavyCtx& hc, cudaStream_t st)
 {
-    const size_t smem = 4 * static_cast<size_t>(P);
-    if (f.mode == PJ_DIGIT_HASH) {
-        PJ_CUDA(set_smem(hist_keys_kernel<K, true>, smem));
-        hist_keys_kernel<K, true><<<items * hsplit, HIST_THREADS, smem, st>>>(keys, n, chunk, items, hsplit, f, P,
-                                                                             counts, totals);
-    } else {
-        PJ_CUDA(set_smem(hist_keys_kernel<K, false>, smem));
-        hist_keys_kernel<K, false><<<items * hsplit, HIST_THREADS, smem, st>>>(keys, n, chunk, items, hsplit, f, P,
-                                                                              counts, totals);
-    }
+    const size_t smem = 4 * static_cast<size_t>((P + 3) & ~3) + (HEAVY ? HeavyTable::BYTES : 0);
+    auto* kern = hist_keys_kernel<K, HASHD, HEAVY>;
+    PJ_CUDA(set_smem(kern, smem));
+    typename HeavyArg<HEAVY>::type h{};
+    if constexpr (HEAVY) h = *hc.hs;
+    kern<<<items * hsplit, HIST_THREADS, smem, st>>>(keys, n, chunk, items, hsplit, f, P, counts, totals, h, hc.out);
     PJ_CUDA(cudaGetLastError());
     return PJ_OK;
+}
+
+// hc.hs: heavy probe keys to leave out (nullptr: none)
+template <typename K>
+pj_status launch_hist(const K* keys, int64_t n, int64_t chunk, int items, int hsplit, DigitFn f, int P,
+                      uint32_t* counts, int32_t* totals, cudaStream_t st, const HeavyCtx& hc = HeavyCtx())
+{
+    const bool hd = f.mode == PJ_DIGIT_HASH;
+    if (hc.hs)
+        return hd ? launch_hist_t<K, true, true>(keys, n, chunk, items, hsplit, f, P, counts, totals, hc, st)
+                  : launch_hist_t<K, false, true>(keys, n, chunk, items, hsplit, f, P, counts, totals, hc, st);
+    return hd ? launch_hist_t<K, true, false>(keys, n, chunk, items, hsplit, f, P, counts, totals, hc, st)
+              : launch_hist_t<K, false, false>(keys, n, chunk, items, hsplit, f, P, counts, totals, hc, st);
 }
 
 template <typename TIn>
@@ -395,35 +425,45 @@ pj_status launch_scan(const TIn* in, int64_t m, uint32_t round_to, int64_t* out,
     return PJ_OK;
 }
 
-template <typename K, int W, bool HASHD>
-pj_status launch_scatter_w(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P,
-                           const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status, cudaStream_t st)
+template <typename K, int W, bool HASHD, bool HEAVY>
+pj_status launch_scatter_t(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P,
+                           const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status,
+                           const HeavyCtx& hc, cudaStream_t st)
 {
-    auto* kern = scatter_keys_kernel<K, SC_THREADS, sc_v<K>(), W, HASHD>;
-    const size_t smem = scatter_smem(sizeof(K), W, P);
+    auto* kern = scatter_keys_kernel<K, SC_THREADS, sc_v<K>(), W, HASHD, HEAVY>;
+    const size_t smem = HEAVY ? heavy_table_offset(P, WcTraits<K, W>::BW) + HeavyTable::BYTES
+                              : scatter_smem(sizeof(K), W, P);
     PJ_CUDA(set_smem(kern, smem));
+    typename HeavyArg<HEAVY>::type h{};
+    if constexpr (HEAVY) h = *hc.hs;
     kern<<<items, SC_THREADS, smem, st>>>(keys, n, chunk, items, f, P, offsets, out,
-                                         static_cast<uint32_t>(std::min<int64_t>(out_cap, UINT32_MAX)), status);
+                                         static_cast<uint32_t>(std::min<int64_t>(out_cap, UINT32_MAX)), status, h,
+                                         hc.out);
     PJ_CUDA(cudaGetLastError());
     return PJ_OK;
 }
 
+template <typename K, int W>
+pj_status launch_scatter_w(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P,
+                           const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status,
+                           const HeavyCtx& hc, cudaStream_t st)
+{
+    const bool hd = f.mode == PJ_DIGIT_HASH;
+    if (hc.hs)
+        return hd ? launch_scatter_t<K, W, true, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st)
+                  : launch_scatter_t<K, W, false, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
+    return hd ? launch_scatter_t<K, W, true, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st)
+              : launch_scatter_t<K, W, false, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
+}
+
 template <typename K>
 pj_status launch_scatter(const K* keys, int64_t n, int64_t chunk, int items, DigitFn f, int P, int W,
-                         const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status, cudaStream_t st)
+                         const int64_t* offsets, uint32_t* out, int64_t out_cap, uint32_t* status, cudaStream_t st,
+                         const HeavyCtx& hc = HeavyCtx())
 {
-    const bool h = f.mode == PJ_DIGIT_HASH;
-    if constexpr (sizeof(K) == 4) {
-        if (W == 2)
-            return h ? launch_scatter_w<K, 2, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st)
-                     : launch_scatter_w<K, 2, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st);
-    }
-    if (W == 4)
-        return h ? launch_scatter_w<K, 4, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st)
-                 : launch_scatter_w<K, 4, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st);
-    if (W == 8)
-        return h ? launch_scatter_w<K, 8, true>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st)
-                 : launch_scatter_w<K, 8, false>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, st);
+    if (W == 2) return launch_scatter_w<K, 2>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
+    if (W == 4) return launch_scatter_w<K, 4>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
+    if (W == 8) return launch_scatter_w<K, 8>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
     return PJ_ERR_INVALID;
 }
 
@@ -440,7 +480,7 @@ pj_status launch_join_t(const JoinArgs& a, cudaStream_t st)
     kern<<<grid, JN_THREADS, smem, st>>>(a);
     PJ_CUDA(cudaGetLastError());
     // fix-up: dense output and the true count
-    join_fixup_plan_kernel<<<1, 1024, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.capacity,
+    join_fixup_plan_kernel<<<1, 1024, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.base_count, a.capacity,
                                                a.out_build != nullptr ? 1 : 0, a.seg, a.status);
     PJ_CUDA(cudaGetLastError());
     if (a.out_build != nullptr) {
@@ -488,7 +528,8 @@ struct StageEvents {
 // Partition one column: histogram -> look-back scan -> scatter.
 template <typename K>
 pj_status partition_column(const K* keys, int64_t n, const pj_plan* p, const Layout& L, int side, uint8_t* ws,
-                           uint32_t* tuples, int64_t cap, const StageEvents& E, int stage0, cudaStream_t st)
+                           uint32_t* tuples, int64_t cap, const StageEvents& E, int stage0, cudaStream_t st,
+                           const HeavyCtx& hc = HeavyCtx())
 {
     const DigitFn f = digit_fn(p->digit_mode, 0, p->bits1, 0);
     const int64_t chunk = side == 0 ? L.b_chunk : L.p_chunk;
@@ -501,13 +542,13 @@ pj_status partition_column(const K* keys, int64_t n, const pj_plan* p, const Lay
     uint64_t* tiles = reinterpret_cast<uint64_t*>(ws + (side == 0 ? L.b_tiles : L.p_tiles));
     pj_status s;
     E.mark(stage0, st);
-    if ((s = launch_hist<K>(keys, n, chunk, items, p->hist_split, f, L.P, counts, tot, st)) != PJ_OK) return s;
+    if ((s = launch_hist<K>(keys, n, chunk, items, p->hist_split, f, L.P, counts, tot, st, hc)) != PJ_OK) return s;
     E.mark(stage0 + 1, st);
     if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(L.P) * items, static_cast<uint32_t>(p->wc_tuples), off,
                                    tiles, ctr + (side == 0 ? CTR_BTILE : CTR_PTILE), status, st)) != PJ_OK)
         return s;
     E.mark(stage0 + 2, st);
-    return launch_scatter<K>(keys, n, chunk, items, f, L.P, p->wc_tuples, off, tuples, cap, status, st);
+    return launch_scatter<K>(keys, n, chunk, items, f, L.P, p->wc_tuples, off, tuples, cap, status, st, hc);
 }
 
 template <typename K>
@@ -524,15 +565,38 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
         return PJ_OK;
     }
     pj_status s;
+    // heavy-key path: unique build keys and a plan that names heavy probe keys
+    HeavySet hs{};
+    HeavyCtx hc;
+    auto* heavy_total = reinterpret_cast<unsigned long long*>(ws + L.heavy_total);
+    if (p->n_heavy > 0 && d->unique_build_keys) {
+        hs.n = p->n_heavy;
+        for (int i = 0; i < p->n_heavy; ++i) hs.keys[i] = p->heavy_keys[i];
+        int32_t* hrow = reinterpret_cast<int32_t*>(ws + L.heavy_row);
+        PJ_CUDA(cudaMemsetAsync(hrow, 0xff, 4 * MAX_HEAVY, st));
+        hc.hs = &hs;
+        hc.out = HeavyOut{hrow, reinterpret_cast<unsigned long long*>(ws + L.heavy_items), out_b, out_p, capacity};
+    }
     if ((s = partition_column<K>(static_cast<const K*>(d->build_keys), d->n_build, p, L, 0, ws,
                                  reinterpret_cast<uint32_t*>(ws + L.b_tuples), L.b_cap, E, PJ_STAGE_BUILD_HIST,
                                  st)) != PJ_OK)
         return s;
+    if (hc.hs) {  // build rows of the heavy keys (timed with the build scatter)
+        heavy_rows_kernel<K><<<static_cast<unsigned>(sm_count()) * 4, 512, 0, st>>>(static_cast<const K*>(d->build_keys),
+                                                                        d->n_build, hs,
+                                                                        const_cast<int32_t*>(hc.out.heavy_row));
+        PJ_CUDA(cudaGetLastError());
+    }
     if ((s = partition_column<K>(static_cast<const K*>(d->probe_keys), d->n_probe, p, L, 1, ws,
                                  reinterpret_cast<uint32_t*>(ws + L.p_tuples), L.p_cap, E, PJ_STAGE_PROBE_HIST,
-                                 st)) != PJ_OK)
+                                 st, hc)) != PJ_OK)
         return s;
     E.mark(PJ_STAGE_JOIN_PLAN, st);
+    if (hc.hs) {  // the heavy pairs [0, H) precede every join chunk
+        heavy_total_kernel<<<1, 32, 0, st>>>(hc.out.item_count, L.p_items, heavy_total,
+                                             reinterpret_cast<unsigned long long*>(count));
+        PJ_CUDA(cudaGetLastError());
+    }
 
     const int cap_tuples = table_tuples(p);
     const bool hash_split = p->split_mode == PJ_SPLIT_HASH;
@@ -581,6 +645,7 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     a.over_probe = reinterpret_cast<int32_t*>(ws + L.over_p);
     a.over_cap = L.over_cap;
     a.max_ctas = L.max_ctas;
+    a.base_count = heavy_total;
     E.mark(PJ_STAGE_JOIN, st);
     s = launch_join<K>(a, p->table_mode, d->unique_build_keys != 0, hash_split, p->slot_mode == PJ_SLOT_REF, st);
     if (s == PJ_OK && out_b && (pay_b || pay_p) && d->payload_bytes > 0) {
@@ -692,12 +757,19 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     p->split_mode = d->unique_build_keys ? PJ_SPLIT_HASH : PJ_SPLIT_POSITION;
     p->max_fill = 0.5f;  // HASH_TABLE_OCC, hash_join_kernels.cuh:21
     p->table_capacity = max_table_capacity(d->key_bytes, p->table_mode);
-    p->probe_chunk = 1 << 16;
+    // Probe tuples per work item: at least 64 K, and large enough that a
+    // partition of average size is one item (every extra item of a partition
+    // rebuilds its table) -- about 8 items per SM over the whole join.  Only
+    // partitions far above average (skewed probe keys) are split.
+    {
+        const int64_t per = (d->n_probe + static_cast<int64_t>(sm_count()) * 8 - 1) / (static_cast<int64_t>(sm_count()) * 8);
+        p->probe_chunk = static_cast<int32_t>(std::min<int64_t>(std::max<int64_t>(1 << 16, (per + 15) / 16 * 16), 1 << 30));
+    }
     p->scatter_ctas_per_sm = 1;
     p->hist_split = 2;
     // Widest write-combining buffer that the shared memory allows at a fan-out.
     auto pick_w = [&](int b) {
-        for (int W : {8, 4})
+        for (int W : {8, 4, 2})
             if (sector_wc(d->key_bytes, W) && scatter_smem(d->key_bytes, W, 1 << b) <= smem_limit() &&
                 (W <= 4 || b <= 8 || d->key_bytes == 8))
                 return W;
@@ -954,20 +1026,56 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
     if ((s = pj_radix_histogram(d->build_keys, d->n_build, d->key_bytes, PJ_DIGIT_HASH, p.bits1, 0, 0, hist + P,
                                 stream)) != PJ_OK)
         return s;
-    int32_t* host = new int32_t[2 * static_cast<size_t>(P)];
-    cudaError_t e = cudaMemcpyAsync(host, hist, sizeof(int32_t) * 2 * P, cudaMemcpyDeviceToHost, st);
+    // A sample of the probe keys for the heavy-key path (unique build keys:
+    // a heavy probe key then has at most one build row).
+    const bool sample = d->unique_build_keys && d->n_probe >= HEAVY_MIN_PROBE;
+    std::vector<int64_t> keys_h(sample ? HEAVY_SAMPLES : 0);
+    int64_t* sample_d = reinterpret_cast<int64_t*>(static_cast<uint8_t*>(ws) + L.sample);
+    if (sample) {
+        if (d->key_bytes == 4)
+            sample_keys_kernel<int32_t><<<HEAVY_SAMPLES / 256, 256, 0, st>>>(
+                static_cast<const int32_t*>(d->probe_keys), d->n_probe, HEAVY_SAMPLES, sample_d);
+        else
+            sample_keys_kernel<int64_t><<<HEAVY_SAMPLES / 256, 256, 0, st>>>(
+                static_cast<const int64_t*>(d->probe_keys), d->n_probe, HEAVY_SAMPLES, sample_d);
+        PJ_CUDA(cudaGetLastError());
+    }
+    std::vector<int32_t> host(2 * static_cast<size_t>(P));
+    cudaError_t e = cudaMemcpyAsync(host.data(), hist, sizeof(int32_t) * 2 * P, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && sample)
+        e = cudaMemcpyAsync(keys_h.data(), sample_d, sizeof(int64_t) * HEAVY_SAMPLES, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
-        delete[] host;
         last_cuda_error() = e;
         return PJ_ERR_CUDA;
+    }
+    if (sample) {
+        // heavy: at least HEAVY_MIN_SAMPLES of the sample (>= 1/2048 of the
+        // probe rows); the most frequent PJ_MAX_HEAVY of them
+        std::unordered_map<int64_t, int> freq;
+        freq.reserve(keys_h.size());
+        for (int64_t k : keys_h) ++freq[k];
+        std::vector<std::pair<int, int64_t>> heavy;
+        for (const auto& kv : freq)
+            if (kv.second >= HEAVY_MIN_SAMPLES) heavy.emplace_back(kv.second, kv.first);
+        std::sort(heavy.begin(), heavy.end(), [](const auto& x, const auto& y) {
+            return x.first != y.first ? x.first > y.first : x.second < y.second;
+        });
+        p.n_heavy = static_cast<int32_t>(std::min<size_t>(heavy.size(), PJ_MAX_HEAVY));
+        int64_t covered = 0;
+        for (int i = 0; i < p.n_heavy; ++i) {
+            p.heavy_keys[i] = heavy[i].second;
+            covered += heavy[i].first;
+        }
+        // the path pays a lookup for every probe key: worth it only when the
+        // heavy keys carry a large share of the probe side
+        if (covered < static_cast<int64_t>(HEAVY_MIN_SHARE * HEAVY_SAMPLES)) p.n_heavy = 0;
     }
     int64_t raw_max = 0, hash_max = 0;
     for (int i = 0; i < P; ++i) {
         raw_max = std::max<int64_t>(raw_max, host[i]);
         hash_max = std::max<int64_t>(hash_max, host[P + i]);
     }
-    delete[] host;
     // Raw key bits are free to compute: keep them (the reference's digits)
     // when their largest partition is no worse than the hashed one's.
     p.digit_mode = raw_max <= hash_max ? PJ_DIGIT_RAW : PJ_DIGIT_HASH;

@@ -99,53 +99,15 @@ __device__ __forceinline__ uint32_t slot_ref(uint32_t h, int32_t T)
 }
 
 // ---------------------------------------------------------------------------
-// Partitioned tuples.  4-byte keys: {key, row} (8 B).  8-byte keys:
-// {key_lo, key_hi, row} (12 B).  Padding tuples have row == -1.
+// Partitioned tuples.  4-byte keys: {murmur(key), row} (8 B).  8-byte keys:
+// {key_lo, key_hi, murmur(key), row} (16 B: one aligned vector, and the join
+// never hashes again).  The row is the last word; padding tuples have
+// row == -1.
 template <typename K> struct TupleTraits;
 template <> struct TupleTraits<int32_t> { static constexpr int WORDS = 2; };
-template <> struct TupleTraits<int64_t> { static constexpr int WORDS = 3; };
+template <> struct TupleTraits<int64_t> { static constexpr int WORDS = 4; };
 
 constexpr int32_t PAD_ROW = -1;
-
-template <typename K>
-__device__ __forceinline__ void load_tuple(const uint32_t* __restrict__ base, int64_t i, K& key, int32_t& row);
-
-template <>
-__device__ __forceinline__ void load_tuple<int32_t>(const uint32_t* __restrict__ base, int64_t i, int32_t& key,
-                                                    int32_t& row)
-{
-    const uint2 v = __ldg(reinterpret_cast<const uint2*>(base) + i);
-    key = static_cast<int32_t>(v.x);
-    row = static_cast<int32_t>(v.y);
-}
-
-template <>
-__device__ __forceinline__ void load_tuple<int64_t>(const uint32_t* __restrict__ base, int64_t i, int64_t& key,
-                                                    int32_t& row)
-{
-    const uint32_t* p = base + 3 * i;
-    const uint32_t lo = __ldg(p), hi = __ldg(p + 1);
-    key = static_cast<int64_t>((static_cast<uint64_t>(hi) << 32) | lo);
-    row = static_cast<int32_t>(__ldg(p + 2));
-}
-
-template <typename K>
-__device__ __forceinline__ void put_tuple_words(uint32_t* dst, K key, int32_t row);
-
-template <>
-__device__ __forceinline__ void put_tuple_words<int32_t>(uint32_t* dst, int32_t key, int32_t row)
-{
-    *reinterpret_cast<uint2*>(dst) = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(row));
-}
-
-template <>
-__device__ __forceinline__ void put_tuple_words<int64_t>(uint32_t* dst, int64_t key, int32_t row)
-{
-    const uint64_t u = static_cast<uint64_t>(key);
-    dst[0] = static_cast<uint32_t>(u);
-    dst[1] = static_cast<uint32_t>(u >> 32);
-    dst[2] = static_cast<uint32_t>(row);
-}
 
 // Bounded spin: iterations before a wait gives up and raises ST_TIMEOUT.
 constexpr uint32_t SPIN_LIMIT = 1u << 24;

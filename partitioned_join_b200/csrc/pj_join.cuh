@@ -83,6 +83,7 @@ struct JoinArgs {
     int64_t over_cap;
     int64_t* seg;               // fix-up segments
     int32_t max_ctas;           // join CTAs the fix-up records have room for
+    const unsigned long long* base_count;  // entries written before the join (heavy keys), or nullptr
 };
 
 // Items per partition (S_p x K_p) and the split of partition p.
@@ -136,9 +137,42 @@ __global__ void items_expand_kernel(const int64_t* __restrict__ item_off, int32_
 }
 
 // ---------------------------------------------------------------------------
+// L2 residency.  Probe tuples and output entries stream through once; the
+// item's build tuples are re-read (place pass, COMPACT verification).  The
+// streams are tagged evict-first so that they do not push the build range
+// out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ uint2 ld_stream(const uint2* p, uint64_t pol)
+{
+    uint2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                 : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ uint4 ld_stream(const uint4* p, uint64_t pol)
+{
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ void st_stream(int32_t* p, int32_t v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
+}
+
+// ---------------------------------------------------------------------------
 // Tuple access: a probe/build tuple gives (hash, comparable key, row).
 // 4-byte keys: the stored word 0 is murmur(key), a bijection, so the hash is
-// the key.  8-byte keys: the key is stored, the hash recomputed.
+// the key.  8-byte keys: the key and its hash are both stored.
 template <typename K> struct TupleView;
 
 template <> struct TupleView<int32_t> {
@@ -147,6 +181,14 @@ template <> struct TupleView<int32_t> {
     __device__ __forceinline__ static void load(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key, int32_t& row)
     {
         const uint2 v = __ldg(reinterpret_cast<const uint2*>(base) + i);
+        h = v.x;
+        key = v.x;
+        row = static_cast<int32_t>(v.y);
+    }
+    __device__ __forceinline__ static void load_stream(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key,
+                                                       int32_t& row, uint64_t pol)
+    {
+        const uint2 v = ld_stream(reinterpret_cast<const uint2*>(base) + i, pol);
         h = v.x;
         key = v.x;
         row = static_cast<int32_t>(v.y);
@@ -160,21 +202,28 @@ template <> struct TupleView<int32_t> {
 };
 
 template <> struct TupleView<int64_t> {
-    static constexpr int WORDS = 3;
+    static constexpr int WORDS = 4;  // {key_lo, key_hi, hash, row}
     using Cmp = unsigned long long;
     __device__ __forceinline__ static void load(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key, int32_t& row)
     {
-        const uint32_t* p = base + 3 * i;
-        const uint32_t lo = __ldg(p), hi = __ldg(p + 1);
-        key = (static_cast<unsigned long long>(hi) << 32) | lo;
-        row = static_cast<int32_t>(__ldg(p + 2));
-        h = hash_key(static_cast<int64_t>(key));
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(base) + i);
+        key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
+        h = v.z;
+        row = static_cast<int32_t>(v.w);
+    }
+    __device__ __forceinline__ static void load_stream(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key,
+                                                       int32_t& row, uint64_t pol)
+    {
+        const uint4 v = ld_stream(reinterpret_cast<const uint4*>(base) + i, pol);
+        key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
+        h = v.z;
+        row = static_cast<int32_t>(v.w);
     }
     __device__ __forceinline__ static void load_key_row(const uint32_t* base, int64_t i, Cmp& key, int32_t& row)
     {
-        const uint32_t* p = base + 3 * i;
-        key = (static_cast<unsigned long long>(__ldg(p + 1)) << 32) | __ldg(p);
-        row = static_cast<int32_t>(__ldg(p + 2));
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(base) + i);
+        key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
+        row = static_cast<int32_t>(v.w);
     }
 };
 
@@ -219,6 +268,20 @@ __device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes)
         const int64_t left = bytes - off;
         const uint32_t n = static_cast<uint32_t>((left < 65536 ? left : 65536) & ~int64_t(15));
         if (n) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + off), "r"(n) : "memory");
+    }
+}
+
+// The same for data read once (probe chunks): tagged evict-first.
+__device__ __forceinline__ void prefetch_l2_stream(const void* p, int64_t bytes, uint64_t pol)
+{
+    const uint8_t* c = static_cast<const uint8_t*>(p);
+    for (int64_t off = 0; off < bytes; off += 65536) {
+        const int64_t left = bytes - off;
+        const uint32_t n = static_cast<uint32_t>((left < 65536 ? left : 65536) & ~int64_t(15));
+        if (n)
+            asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(c + off), "r"(n),
+                         "l"(pol)
+                         : "memory");
     }
 }
 
@@ -321,6 +384,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     __shared__ int s_nbuild;
     __shared__ uint32_t s_step;  // next probe step of the current item
 
+    const uint64_t stream_pol = l2_evict_first_policy();
     const int NB = 1 << a.nb_log2;
     const uint32_t nb_mask = static_cast<uint32_t>(NB - 1);
     const int64_t total_items = a.item_off[a.P];
@@ -405,8 +469,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             int32_t* ob = a.out_build + b0 + off0;
             int32_t* op = a.out_probe + b0 + off0;
             for (int i = lane; i < n0; i += 32) {
-                ob[i] = stage_b[i];
-                op[i] = stage_p[i];
+                st_stream(ob + i, stage_b[i], stream_pol);
+                st_stream(op + i, stage_p[i], stream_pol);
             }
         } else {
             for (int i = lane; i < n0; i += 32)
@@ -453,7 +517,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         const int64_t q_hi = q_lo + a.probe_chunk < q_hi0 ? q_lo + a.probe_chunk : q_hi0;
 
         // the probe chunk streams into L2 while the table is built
-        if (threadIdx.x == 0) prefetch_l2(a.probe_tuples + (q_lo * TV::WORDS), (q_hi - q_lo) * TV::WORDS * 4);
+        if (threadIdx.x == 0)
+            prefetch_l2_stream(a.probe_tuples + (q_lo * TV::WORDS), (q_hi - q_lo) * TV::WORDS * 4, stream_pol);
 
         auto in_piece = [&](uint32_t h) -> bool {
             if (!HASH_SPLIT || sbits == 0) return true;
@@ -607,7 +672,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                 for (int u = 0; u < U; ++u) {
                     const uint32_t i = s0 + u * 32 + lane;
                     nr[u] = -1;
-                    if (i < qn) TV::load(pbase, i, nh[u], nk[u], nr[u]);
+                    if (i < qn) TV::load_stream(pbase, i, nh[u], nk[u], nr[u], stream_pol);
                 }
             };
             uint32_t s0 = claim();
@@ -909,7 +974,9 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 // hole (start, prefix) pairs, then mover (start, prefix) pairs.
 __global__ void __launch_bounds__(1024) join_fixup_plan_kernel(const int64_t* __restrict__ cta_q,
                                                                const int64_t* __restrict__ cta_last, int32_t n_cta,
-                                                               unsigned long long* count, int64_t capacity,
+                                                               unsigned long long* count,
+                                                               const unsigned long long* __restrict__ base_count,
+                                                               int64_t capacity,
                                                                int32_t write_out, int64_t* __restrict__ seg,
                                                                uint32_t* __restrict__ status)
 {
@@ -946,7 +1013,7 @@ __global__ void __launch_bounds__(1024) join_fixup_plan_kernel(const int64_t* __
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const long long total = s_sum;
+        const long long total = s_sum + (base_count ? static_cast<long long>(*base_count) : 0);
         const long long reserved = static_cast<long long>(*count);
         *count = static_cast<unsigned long long>(total);
         int nh = 0, nm = 0;

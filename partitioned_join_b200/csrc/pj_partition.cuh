@@ -14,20 +14,25 @@
 // of a 4-byte key is a bijection of 32-bit values (every step -- odd
 // multiplies, rotations, xor/add of constants, the fmix32 xor-shifts -- is
 // invertible), so equal hashes mean equal keys and the join never hashes
-// again.  8-byte keys are stored as {key_lo, key_hi, row}.
+// again.  8-byte keys are stored as {key_lo, key_hi, murmur(key), row}.
 //
 // Reference counterparts: histogram_pass_one (partition_kernels.cuh:141-194),
 // the ExclusiveSum + copy of partitioned_join.cuh:86-88, partition_pass_one
 // (partition_kernels.cuh:197-326).  The reference stages an 8 192-key tile in
 // shared memory and flushes each partition's run with 32 threads; here each
 // CTA keeps a W-tuple write-combining buffer per partition and writes only
-// whole, aligned W-tuple groups, so the fan-out of one pass can be 8 192.
+// whole, aligned W-tuple groups (32-byte sectors), so the fan-out of one pass
+// reaches 4 096.
+//
+// With the heavy-key path (pj_heavy.cuh) the probe side's histogram skips
+// heavy keys and its scatter writes their output pairs directly.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "pj_device.cuh"
+#include "pj_heavy.cuh"
 
 namespace pj {
 
@@ -53,6 +58,25 @@ __device__ __forceinline__ void load_vec16(const K* p, K (&out)[Vec16<K>::N])
     }
 }
 
+// Byte offset of the heavy table in the scatter's shared memory: after P
+// buffers of BW words and P {fill, cursor} pairs, rounded up to 16 bytes.
+__host__ __device__ constexpr size_t heavy_table_offset(int P, int BW)
+{
+    return (static_cast<size_t>(P) * BW * 4 + static_cast<size_t>(P) * 8 + 15) & ~static_cast<size_t>(15);
+}
+
+// Output of heavy probe keys (heavy-key path).  The probe histogram counts,
+// per item, the heavy probe rows that have a build row; item i's pairs then
+// go to [sum of the counts of items < i, ...) -- exact positions, no global
+// atomics -- and the join's output starts after all of them.
+struct HeavyOut {
+    const int32_t* heavy_row;          // build row of each heavy key (-1: none)
+    unsigned long long* item_count;    // per scatter item: heavy pairs (zeroed by the caller)
+    int32_t* out_build;                // nullptr: count only
+    int32_t* out_probe;
+    int64_t capacity;
+};
+
 // ---------------------------------------------------------------------------
 // Histogram.  Grid = n_items * hsplit CTAs; CTA c counts the keys of the
 // (c % hsplit)-th slice of item c / hsplit's chunk in shared memory and adds
@@ -60,17 +84,24 @@ __device__ __forceinline__ void load_vec16(const K* p, K (&out)[Vec16<K>::N])
 constexpr int HIST_THREADS = 512;
 constexpr int HIST_UNROLL = 4;  // 16-byte vectors in flight per thread
 
-template <typename K, bool HASHD>
+template <typename K, bool HASHD, bool HEAVY>
 __global__ void __launch_bounds__(HIST_THREADS) hist_keys_kernel(const K* __restrict__ keys, int64_t n,
                                                                  int64_t chunk, int32_t n_items, int32_t hsplit,
                                                                  DigitFn f, int32_t P,
                                                                  uint32_t* __restrict__ counts_T,
-                                                                 int32_t* __restrict__ totals)
+                                                                 int32_t* __restrict__ totals,
+                                                                 typename HeavyArg<HEAVY>::type hs, HeavyOut ho)
 {
     constexpr int VN = Vec16<K>::N;
     extern __shared__ __align__(16) uint32_t cnt[];
     const int item = blockIdx.x / hsplit, part = blockIdx.x % hsplit;
     for (int p = threadIdx.x; p < P; p += HIST_THREADS) cnt[p] = 0;
+    HeavyTable heavy;
+    uint32_t heavy_hits = 0;
+    if constexpr (HEAVY) {
+        heavy.bind(reinterpret_cast<uint8_t*>(cnt + ((P + 3) & ~3)));
+        heavy.build<K>(hs, ho.heavy_row);  // ends with a barrier
+    }
     __syncthreads();
     int64_t lo = static_cast<int64_t>(item) * chunk;
     int64_t hi = lo + chunk < n ? lo + chunk : n;
@@ -80,10 +111,23 @@ __global__ void __launch_bounds__(HIST_THREADS) hist_keys_kernel(const K* __rest
     int64_t s_lo = lo + part * per;
     int64_t s_hi = s_lo + per < hi ? s_lo + per : hi;
     if (s_lo > s_hi) s_lo = s_hi;
+    // digit of key k, or -1 for a heavy probe key (not partitioned)
+    auto digit = [&](K k) -> int {
+        if constexpr (HEAVY) {
+            const HeavyHit e = heavy.find(k);
+            if (e.idx >= 0) {
+                heavy_hits += e.row >= 0 ? 1u : 0u;
+                return -1;
+            }
+        }
+        uint32_t h = 0;
+        if constexpr (HASHD) h = hash_key(k);
+        return static_cast<int>(HASHD ? ((h >> f.shift) & f.mask)
+                                      : (static_cast<uint32_t>(static_cast<uint64_t>(k) >> f.shift) & f.mask));
+    };
     auto count = [&](K k) {
-        const uint32_t d = HASHD ? ((hash_key(k) >> f.shift) & f.mask)
-                                 : (static_cast<uint32_t>(static_cast<uint64_t>(k) >> f.shift) & f.mask);
-        atomicAdd(&cnt[d], 1u);
+        const int d = digit(k);
+        if (d >= 0) atomicAdd(&cnt[d], 1u);
     };
     constexpr int STEP = HIST_THREADS * VN * HIST_UNROLL;
     int64_t base = s_lo;
@@ -98,6 +142,10 @@ __global__ void __launch_bounds__(HIST_THREADS) hist_keys_kernel(const K* __rest
             for (int e = 0; e < VN; ++e) count(v[u][e]);
     }
     for (int64_t i = base + threadIdx.x; i < s_hi; i += HIST_THREADS) count(keys[i]);
+    if constexpr (HEAVY) {
+        heavy_hits = __reduce_add_sync(0xffffffffu, heavy_hits);
+        if ((threadIdx.x & 31) == 0 && heavy_hits) atomicAdd(&ho.item_count[item], static_cast<unsigned long long>(heavy_hits));
+    }
     __syncthreads();
     for (int p = threadIdx.x; p < P; p += HIST_THREADS) {
         const uint32_t c = cnt[p];
@@ -267,12 +315,13 @@ __device__ __forceinline__ void tuple_words<int32_t>(uint32_t (&w)[2], int32_t k
 }
 
 template <>
-__device__ __forceinline__ void tuple_words<int64_t>(uint32_t (&w)[3], int64_t key, int32_t row)
+__device__ __forceinline__ void tuple_words<int64_t>(uint32_t (&w)[4], int64_t key, int32_t row)
 {
     const uint64_t u = static_cast<uint64_t>(key);
     w[0] = static_cast<uint32_t>(u);
     w[1] = static_cast<uint32_t>(u >> 32);
-    w[2] = static_cast<uint32_t>(row);
+    w[2] = hash_key(key);  // stored hash: digits, buckets and fingerprints come from it
+    w[3] = static_cast<uint32_t>(row);
 }
 
 template <int TW>
@@ -280,6 +329,8 @@ __device__ __forceinline__ void store_words(uint32_t* dst, const uint32_t (&w)[T
 {
     if constexpr (TW == 2) {
         *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
+    } else if constexpr (TW == 4) {
+        *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
     } else {
 #pragma unroll
         for (int i = 0; i < TW; ++i) dst[i] = w[i];
@@ -312,24 +363,19 @@ __device__ __forceinline__ void wc_flush(const uint32_t* sbuf, uint32_t* gdst)
     }
 }
 
-template <typename K, int THREADS, int V, int W>
-struct ScatterSmem {
-    static size_t bytes(int P)
-    {
-        return static_cast<size_t>(P) * WcTraits<K, W>::BW * 4 + static_cast<size_t>(P) * 8;
-    }
-};
+
 
 // Scatter of a raw key column (row = key index).  V keys per thread per
 // round (whole 16-byte vectors), the next two rounds' vectors loaded while
 // the current round is processed.  Per partition the CTA keeps a W-tuple
 // buffer and a packed {fill, cursor} pair (one 64-bit shared access).
-template <typename K, int THREADS, int V, int W, bool HASHD>
+template <typename K, int THREADS, int V, int W, bool HASHD, bool HEAVY>
 __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __restrict__ keys, int64_t n,
                                                                   int64_t chunk, int32_t n_items, DigitFn f,
                                                                   int32_t P, const int64_t* __restrict__ offsets,
                                                                   uint32_t* __restrict__ out, uint32_t out_cap,
-                                                                  uint32_t* __restrict__ status)
+                                                                  uint32_t* __restrict__ status,
+                                                                  typename HeavyArg<HEAVY>::type hs, HeavyOut ho)
 {
     constexpr int TW = WcTraits<K, W>::TW, BW = WcTraits<K, W>::BW;
     constexpr int VN = Vec16<K>::N;
@@ -339,10 +385,31 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __res
     extern __shared__ __align__(128) uint8_t smem[];
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
     int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * BW);  // {fill, cursor}
+    HeavyTable heavy;
+    if constexpr (HEAVY) {
+        // after the buffers and counters, on a 16-byte boundary (slots are
+        // read as 16-byte words)
+        heavy.bind(smem + heavy_table_offset(P, BW));
+        heavy.build<K>(hs, ho.heavy_row);  // ends with a barrier
+    }
+    const int lane = threadIdx.x & 31;
 
+    __shared__ unsigned long long s_hbase;  // heavy pairs of the items before this one
+    __shared__ uint32_t s_hcur;             // heavy pairs of this item so far
     for (int32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         for (int p = threadIdx.x; p < P; p += THREADS)
             fc[p] = make_int2(0, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
+        if constexpr (HEAVY) {
+            if (threadIdx.x < 32) {
+                unsigned long long sum = 0;
+                for (int j = threadIdx.x; j < item; j += 32) sum += ho.item_count[j];
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+                if (threadIdx.x == 0) {
+                    s_hbase = sum;
+                    s_hcur = 0;
+                }
+            }
+        }
         __syncthreads();
         int64_t lo = static_cast<int64_t>(item) * chunk;
         const int64_t hi = lo + chunk < n ? lo + chunk : n;
@@ -395,13 +462,57 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __res
                     tuple_words<K>(w[v], k, static_cast<int32_t>(row0 + at));
                     uint32_t d;
                     if constexpr (HASHD) {
-                        const uint32_t h = sizeof(K) == 4 ? w[v][0] : hash_key(k);
+                        const uint32_t h = sizeof(K) == 4 ? w[v][0] : w[v][TW - 2];
                         d = (h >> f.shift) & f.mask;
                     } else {
                         d = static_cast<uint32_t>(static_cast<uint64_t>(k) >> f.shift) & f.mask;
                     }
                     dv[v] = d;
                 }
+            if constexpr (HEAVY) {
+                // heavy probe keys: out of the partitions, matched here
+                int32_t hb[V];
+                int c = 0;
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    hb[v] = -1;
+                    if (ok[v]) {
+                        const HeavyHit e = heavy.find(static_cast<K>(cur[v / VN][v % VN]));
+                        if (e.idx >= 0) {
+                            ok[v] = false;
+                            hb[v] = e.row;
+                            c += hb[v] >= 0 ? 1 : 0;
+                        }
+                    }
+                }
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int tot = __shfl_sync(0xffffffffu, incl, 31);
+                if (tot > 0) {
+                    uint32_t base = 0;
+                    if (lane == 31) base = atomicAdd(&s_hcur, static_cast<uint32_t>(tot));
+                    base = __shfl_sync(0xffffffffu, base, 31);
+                    if (ho.out_build) {
+                        long long pos = static_cast<long long>(s_hbase) + base + (incl - c);
+#pragma unroll
+                        for (int v = 0; v < V; ++v) {
+                            if (hb[v] >= 0) {
+                                if (pos < ho.capacity) {
+                                    ho.out_build[pos] = hb[v];
+                                    ho.out_probe[pos] = static_cast<int32_t>(w[v][TW - 1]);
+                                } else {
+                                    raise_status(status, ST_CAPACITY);
+                                }
+                                ++pos;
+                            }
+                        }
+                    }
+                }
+            }
             // phase A
 #pragma unroll
             for (int v = 0; v < V; ++v) {

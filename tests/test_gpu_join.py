@@ -92,7 +92,7 @@ def test_partition_stage_exact(dtype, bits, mode):
     tuples, offsets = api.partition(dev(keys), plan)
     t = tuples.cpu().numpy()
     off = offsets.cpu().numpy()
-    words = 2 if dtype == np.int32 else 3
+    words = 2 if dtype == np.int32 else 4
     P = 1 << bits
     assert off[0] == 0 and np.all(np.diff(off) >= 0)
     rec = t[: off[-1] * words].reshape(-1, words)
@@ -105,6 +105,7 @@ def test_partition_stage_exact(dtype, bits, mode):
     else:
         k = (rec[:, 1].astype(np.int64) << 32) | (rec[:, 0].astype(np.int64) & 0xFFFFFFFF)
         assert np.array_equal(k[real], keys[rows[real]])
+        assert np.array_equal(rec[real, 2].astype(np.uint32), oracle.hash_keys(keys[rows[real]]))
     assert np.all(rows[~real] == -1)
     # every input row exactly once
     assert np.array_equal(np.sort(rows[real]), np.arange(n))
