@@ -263,6 +263,51 @@ pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_
                        void* tuples, int64_t* offsets, void* workspace, size_t workspace_bytes,
                        pj_stream stream);
 
+/* ---- batches of joins (no reference counterpart: the reference runs one
+ * join per process) --------------------------------------------------------
+ * Joins whose build side fits one shared-memory table skip partitioning: one
+ * persistent kernel drains a (join, probe chunk) work queue over all of
+ * them, writing each join's pairs densely to its own output.  Larger joins
+ * take the partitioned path, one after another in a reused workspace
+ * region.  All joins of a batch have the same key width. */
+typedef struct pj_batch_config {
+    int32_t direct_threads;    /* threads per CTA of the direct kernel: 256, 512 or 1024 */
+    int32_t direct_chunk;      /* probe rows per direct work item (>= 1024) */
+    int32_t direct_max_build;  /* joins with at most this many build rows go direct (<= 40960) */
+    int32_t large_bits_delta;  /* added to the default radix bits of the partitioned joins */
+} pj_batch_config;
+
+/* Defaults for a key width. */
+pj_status pj_batch_config_default(int32_t key_bytes, pj_batch_config* cfg);
+
+/* Workspace bytes for the batch under cfg (NULL: defaults). */
+pj_status pj_batch_workspace_size(const pj_join_desc* descs, int32_t n, const pj_batch_config* cfg,
+                                  size_t* bytes);
+
+/* Writes the batch's work table into the workspace (SYNCHRONISES).  Call it
+ * again whenever descs, outs or cfg change. */
+pj_status pj_batch_prepare(const pj_join_desc* descs, const pj_output* outs, int32_t n,
+                           const pj_batch_config* cfg, void* workspace, size_t workspace_bytes,
+                           pj_stream stream);
+
+/* Runs every join of a prepared batch; outs[i] receives join i's pairs and
+ * count.  Asynchronous and free of host synchronisation, so it can be
+ * captured in a CUDA graph and replayed.  Device conditions of any join
+ * (capacity, overflow) come back from pj_batch_check. */
+pj_status pj_join_batch(const pj_join_desc* descs, const pj_output* outs, int32_t n, const pj_batch_config* cfg,
+                        void* workspace, size_t workspace_bytes, pj_stream stream);
+
+/* SYNCHRONISES; returns and clears the batch's device status. */
+pj_status pj_batch_check(void* workspace, pj_stream stream);
+
+/* Autotuner: times candidate configurations on this batch (where the
+ * direct path ends, the direct kernel's block size and chunk, the radix
+ * width of the partitioned joins) and returns the fastest in *best (and its
+ * time, optional).  SYNCHRONISES; runs the batch many times.  The workspace
+ * must hold pj_batch_workspace_size for direct_max_build = 0. */
+pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, int32_t n, void* workspace,
+                            size_t workspace_bytes, pj_stream stream, pj_batch_config* best, float* best_ms);
+
 /* Seeded input tables generated on the device: the reference's
  * generate_input_tables (generate_input_tables.cuh:143-226) and its Zipf
  * generator (generate_zipf_input.cuh:50-134).  Build keys lie in

@@ -57,6 +57,14 @@ class Plan(ctypes.Structure):
         return "Plan(" + ", ".join(f"{k}={v}" for k, v in self.as_dict().items()) + ")"
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("direct_threads", ctypes.c_int32), ("direct_chunk", ctypes.c_int32),
+                ("direct_max_build", ctypes.c_int32), ("large_bits_delta", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # every symbol include/pj.h declares, with its ctypes signature
 _P, _I32, _I64, _SZ = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
 SIGNATURES = {
@@ -78,6 +86,16 @@ SIGNATURES = {
     "pj_radix_histogram": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _I32, _P, _P]),
     "pj_partition": (ctypes.c_int, [_P, _I64, _I32, ctypes.POINTER(Plan), _P, _P, _P, _SZ, _P]),
     "pj_partitioned_capacity": (ctypes.c_int, [_I64, _I32, ctypes.POINTER(Plan), ctypes.POINTER(_I64)]),
+    "pj_batch_config_default": (ctypes.c_int, [_I32, ctypes.POINTER(BatchConfig)]),
+    "pj_batch_workspace_size": (ctypes.c_int, [ctypes.POINTER(JoinDesc), _I32, ctypes.POINTER(BatchConfig),
+                                               ctypes.POINTER(_SZ)]),
+    "pj_batch_prepare": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Output), _I32,
+                                        ctypes.POINTER(BatchConfig), _P, _SZ, _P]),
+    "pj_join_batch": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Output), _I32,
+                                     ctypes.POINTER(BatchConfig), _P, _SZ, _P]),
+    "pj_batch_check": (ctypes.c_int, [_P, _P]),
+    "pj_batch_autotune": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Output), _I32, _P, _SZ, _P,
+                                         ctypes.POINTER(BatchConfig), ctypes.POINTER(ctypes.c_float)]),
     "pj_generate_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I64, ctypes.c_double, _I32, ctypes.c_double,
                                           ctypes.c_uint64, _P, _P]),
 }

@@ -247,6 +247,100 @@ def generate_tables(n_build: int, n_probe: int, key_dtype=torch.int32, rand_max:
     return b, p, int(hits.item())
 
 
+class BatchJoiner:
+    """A batch of joins (pj_join_batch): joins whose build side fits one
+    shared-memory table run in one persistent launch draining a (join, probe
+    chunk) queue; the others take the partitioned path.  Outputs and the
+    workspace are allocated once; launch() only enqueues kernels, so it can
+    be captured in a CUDA graph (see graph())."""
+
+    def __init__(self, pairs, unique_build_keys: bool = True, config: Optional[_lib.BatchConfig] = None):
+        self.pairs = [(_keys(b, "build_keys"), _keys(p, "probe_keys")) for b, p in pairs]
+        n = len(self.pairs)
+        self.n = n
+        dev = self.pairs[0][0].device
+        kb = KEY_DTYPES[self.pairs[0][0].dtype]
+        self.descs = (JoinDesc * n)(*[make_desc(b, p, unique_build_keys) for b, p in self.pairs])
+        self.config = config if config is not None else batch_config_default(kb)
+        self.capacity = [int(p.numel()) if unique_build_keys else join_count(b, p, False) for b, p in self.pairs]
+        self.build_row = [torch.empty(max(c, 1), dtype=torch.int32, device=dev) for c in self.capacity]
+        self.probe_row = [torch.empty(max(c, 1), dtype=torch.int32, device=dev) for c in self.capacity]
+        self.count = torch.zeros(n, dtype=torch.int64, device=dev)
+        outs = []
+        for i in range(n):
+            o = Output()
+            o.build_row, o.probe_row = self.build_row[i].data_ptr(), self.probe_row[i].data_ptr()
+            o.capacity, o.count = self.capacity[i], self.count.data_ptr() + 8 * i
+            outs.append(o)
+        self.outs = (Output * n)(*outs)
+        # room for every configuration the autotuner may try (all joins partitioned)
+        worst = _lib.BatchConfig.from_buffer_copy(self.config)
+        worst.direct_max_build = 0
+        self.ws_bytes = max(self._ws_size(self.config), self._ws_size(worst))
+        for d in (-1, 1):
+            c = _lib.BatchConfig.from_buffer_copy(worst)
+            c.large_bits_delta = d
+            try:
+                self.ws_bytes = max(self.ws_bytes, self._ws_size(c))
+            except PJError:
+                pass
+        self.ws = alloc_workspace(self.ws_bytes, dev)
+        self.prepare()
+
+    def _ws_size(self, cfg) -> int:
+        nb = ctypes.c_size_t(0)
+        check(lib().pj_batch_workspace_size(self.descs, self.n, ctypes.byref(cfg), ctypes.byref(nb)),
+              "pj_batch_workspace_size")
+        return nb.value
+
+    def prepare(self, stream=None) -> None:
+        check(lib().pj_batch_prepare(self.descs, self.outs, self.n, ctypes.byref(self.config),
+                                     ctypes.c_void_p(self.ws.data_ptr()), self.ws_bytes, _stream_ptr(stream)),
+              "pj_batch_prepare")
+
+    def launch(self, stream=None) -> None:
+        check(lib().pj_join_batch(self.descs, self.outs, self.n, ctypes.byref(self.config),
+                                  ctypes.c_void_p(self.ws.data_ptr()), self.ws_bytes, _stream_ptr(stream)),
+              "pj_join_batch")
+
+    def check(self, stream=None) -> None:
+        check(lib().pj_batch_check(ctypes.c_void_p(self.ws.data_ptr()), _stream_ptr(stream)), "pj_join_batch")
+
+    def autotune(self, stream=None) -> float:
+        best = _lib.BatchConfig()
+        ms = ctypes.c_float(0)
+        check(lib().pj_batch_autotune(self.descs, self.outs, self.n, ctypes.c_void_p(self.ws.data_ptr()),
+                                      self.ws_bytes, _stream_ptr(stream), ctypes.byref(best), ctypes.byref(ms)),
+              "pj_batch_autotune")
+        self.config = best
+        self.prepare(stream)
+        return ms.value
+
+    def graph(self):
+        """A CUDA graph of one launch() (replay with .replay())."""
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.launch(s)  # warm-up outside capture: kernel attributes, module loads
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.launch()
+        return g
+
+    def results(self):
+        self.check()
+        counts = self.count.cpu().tolist()
+        return [(self.build_row[i][: counts[i]], self.probe_row[i][: counts[i]]) for i in range(self.n)]
+
+
+def batch_config_default(key_bytes: int = 4) -> _lib.BatchConfig:
+    c = _lib.BatchConfig()
+    check(lib().pj_batch_config_default(key_bytes, ctypes.byref(c)), "pj_batch_config_default")
+    return c
+
+
 def inner_join_noalloc(build_keys: torch.Tensor, probe_keys: torch.Tensor, capacity: int,
                        unique_build_keys: bool = True, plan: Optional[Plan] = None,
                        stream=None) -> Tuple[torch.Tensor, torch.Tensor]:

@@ -109,6 +109,49 @@ template <> struct TupleTraits<int64_t> { static constexpr int WORDS = 4; };
 
 constexpr int32_t PAD_ROW = -1;
 
+// ---------------------------------------------------------------------------
+// Exclusive scan, in place, of the 16-bit counts packed two per word in
+// w[0 .. nwords).  Totals stay below 65536.  Ends with __syncthreads().
+template <int THREADS>
+__device__ __forceinline__ void scan_u16_pairs(uint32_t* w, int nwords, uint32_t* s_warp)
+{
+    const int per = (nwords + THREADS - 1) / THREADS;
+    const int a = threadIdx.x * per;
+    const int b = a + per < nwords ? a + per : nwords;
+    uint32_t sum = 0;
+    for (int i = a; i < b; ++i) {
+        const uint32_t x = w[i];
+        sum += (x & 0xffffu) + (x >> 16);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t x = lane < THREADS / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < THREADS / 32) s_warp[lane] = x;
+    }
+    __syncthreads();
+    uint32_t run = incl - sum + (warp > 0 ? s_warp[warp - 1] : 0u);
+    for (int i = a; i < b; ++i) {
+        const uint32_t x = w[i];
+        const uint32_t c0 = x & 0xffffu, c1 = x >> 16;
+        w[i] = (run & 0xffffu) | ((run + c0) << 16);
+        run += c0 + c1;
+    }
+    __syncthreads();
+}
+
 // Bounded spin: iterations before a wait gives up and raises ST_TIMEOUT.
 constexpr uint32_t SPIN_LIMIT = 1u << 24;
 
