@@ -46,8 +46,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["cfg2", "cfg3"], default="cfg2",
-                    help="cfg2: 2^27 x 2^27 int32 uniform (the headline); cfg3: 2^26 x 2^28 int64, Zipf probe keys")
+    ap.add_argument("--workload", choices=["cfg2", "cfg3", "cfg5"], default="cfg2",
+                    help="cfg2: 2^27 x 2^27 int32 uniform (the headline); cfg3: 2^26 x 2^28 int64, Zipf probe "
+                         "keys; cfg5: 512 int32 joins of uneven sizes, batched against one after another")
+    ap.add_argument("--batch", type=int, default=512, help="cfg5: joins in the batch")
     ap.add_argument("--zipf", type=float, default=1.0, help="cfg3: Zipf exponent of the probe keys")
     ap.add_argument("--log2-build", type=int, default=None)
     ap.add_argument("--log2-probe", type=int, default=None)
@@ -394,11 +396,105 @@ def cpu_baseline(args):
                       f"inner_join_cpu's own timer (build + probe)"}
 
 
+def run_batch(args, rank, world, local):
+    """cfg5: a batch of int32 joins, build sizes log-uniform in 2^10..2^20
+    (unique keys), probe sizes 4x, 70 % uniform matches, every fourth join
+    with Zipf(1.0) probe keys -- run one after another with the plain
+    method, then as one batch (default, autotuned, autotuned in a CUDA
+    graph).  value = batch input tuples/s of the fastest batched form."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from partitioned_join_b200 import _lib, api
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    rng = np.random.default_rng(args.seed + 1000003 * rank)
+    pairs, expected = [], []
+    for i in range(args.batch):
+        nb = int(2 ** rng.uniform(10, 20))
+        b, p, hits = api.generate_tables(nb, 4 * nb, torch.int32, nb - 1, 0.7, True, 1.0 if i % 4 == 3 else 0.0,
+                                         args.seed * 7919 + i, device)
+        pairs.append((b, p))
+        expected.append(hits)
+    tuples = sum(b.numel() + p.numel() for b, p in pairs)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    # plain: pj_inner_join per join, default plan, one reused workspace
+    descs = [api.make_desc(b, p, True) for b, p in pairs]
+    plans = [api.plan_default(d.n_build, d.n_probe, 4, True) for d in descs]
+    ws_bytes = max(api.workspace_size(d, pl) for d, pl in zip(descs, plans))
+    ws = api.alloc_workspace(ws_bytes, device)
+    outs, keep = [], []
+    counts = torch.zeros(len(pairs), dtype=torch.int64, device=device)
+    for i, (b, p) in enumerate(pairs):
+        br = torch.empty(max(p.numel(), 1), dtype=torch.int32, device=device)
+        pr = torch.empty_like(br)
+        keep += [br, pr]
+        o = _lib.Output()
+        o.build_row, o.probe_row, o.capacity, o.count = br.data_ptr(), pr.data_ptr(), p.numel(), counts.data_ptr() + 8 * i
+        outs.append(o)
+    L = _lib.lib()
+
+    def plain():
+        for d, pl, o in zip(descs, plans, outs):
+            _lib.check(L.pj_inner_join(ctypes.byref(d), ctypes.byref(pl), ctypes.byref(o),
+                                       ctypes.c_void_p(ws.data_ptr()), ws_bytes, api._stream_ptr(None)))
+
+    steps = max(1, min(args.steps, 5))
+    plain_ms = timed(plain, steps)
+    _lib.check(L.pj_check(ctypes.c_void_p(ws.data_ptr()), None))
+    plain_ok = counts.cpu().tolist() == expected
+
+    bj = api.BatchJoiner(pairs)
+    default_cfg = bj.config.as_dict()
+    batch_ms = timed(bj.launch, steps)
+    bj.check()
+    batch_ok = bj.count.cpu().tolist() == expected
+    tuned_ms_est = bj.autotune()
+    tuned_ms = timed(bj.launch, steps)
+    g = bj.graph()
+    graph_ms = timed(g.replay, steps)
+    bj.check()
+    graph_ok = bj.count.cpu().tolist() == expected
+    best_ms = min(batch_ms, tuned_ms, graph_ms)
+    line = {
+        "metric": "tuples/s, 512-join uneven batch (cfg5)", "value": tuples / (best_ms / 1e3), "unit": UNIT,
+        "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": best_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"{args.batch} int32 joins, build log-uniform 2^10..2^20 unique, probe 4x, 70% "
+                               f"matches, every fourth Zipf(1.0) (generated on the device)",
+                   "input_tuples": tuples, "batch_default_config": default_cfg, "batch_tuned_config": bj.config.as_dict()},
+        "makespan_ms": {"one_after_another_plain": plain_ms, "batch_default": batch_ms, "batch_autotuned": tuned_ms,
+                        "batch_autotuned_graph": graph_ms, "autotuner_estimate": tuned_ms_est},
+        "speedup_vs_plain": plain_ms / best_ms,
+        "verified": {"plain": plain_ok, "batch": batch_ok, "graph": graph_ok},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "cfg5":
+        run_batch(args, rank, world, local)
     else:
         run_ours(args, rank, world, local)
 
