@@ -308,6 +308,66 @@ pj_status pj_batch_check(void* workspace, pj_stream stream);
 pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, int32_t n, void* workspace,
                             size_t workspace_bytes, pj_stream stream, pj_batch_config* best, float* best_ms);
 
+/* ---- learned planner (no reference counterpart) ----------------------------
+ * A small MLP ranks PJ_PLAN_CANDIDATES schedules of a join -- table layout
+ * (BUCKET or COMPACT) x radix bits (the default -1, 0, +1) x heavy-key path
+ * (off, on) -- from a sketch of a probe-key sample and the sizes.  It only
+ * chooses the schedule: results are those of any plan, and a choice that
+ * overflows a table on the device is rerun with pj_plan_exact by the caller
+ * (PJ_ERR_OVERFLOW from pj_check). */
+#define PJ_MLP_FEATURES 32
+#define PJ_MLP_HIDDEN 64
+#define PJ_PLAN_CANDIDATES 12
+
+/* Shape of an MLP: in -> h1 (ReLU) -> h2 (ReLU) -> out.  Parameters are one
+ * float vector W1[in][h1], b1, W2[h1][h2], b2, W3[h2][out], b3. */
+typedef struct pj_mlp_dims {
+    int32_t in, h1, h2, out;
+} pj_mlp_dims;
+
+/* Number of parameters (floats), or -1. */
+int64_t pj_mlp_param_count(const pj_mlp_dims* dims);
+
+/* y[batch][out] = MLP(x[batch][in]); acts (batch x (2 h1 + 2 h2) floats)
+ * receives the hidden activations for pj_mlp_backward.  Device pointers. */
+pj_status pj_mlp_forward(const float* params, const pj_mlp_dims* dims, const float* x, int32_t batch, float* acts,
+                         float* y, pj_stream stream);
+
+/* grad (param_count floats) = d(loss)/d(params) given dy = d(loss)/dy of a
+ * forward pass on x with activations acts; scratch: batch x (h1 + h2)
+ * floats.  Device pointers. */
+pj_status pj_mlp_backward(const float* params, const pj_mlp_dims* dims, const float* x, const float* acts,
+                          const float* dy, int32_t batch, float* grad, float* scratch, pj_stream stream);
+
+/* Masked mean squared error of y against target (mask NULL: all ones):
+ * dy and the loss (device float, optional).  Device pointers. */
+pj_status pj_mlp_mse_grad(const float* y, const float* target, const float* mask, int64_t n, float* dy, float* loss,
+                          pj_stream stream);
+
+/* One Adam step (step counts from 1).  Device pointers. */
+pj_status pj_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t n, float lr, float beta1,
+                      float beta2, float eps, int32_t step, pj_stream stream);
+
+/* The planner's input: PJ_MLP_FEATURES floats (host) from a sample of the
+ * probe keys (1 % of the rows, 4 096 .. 65 536), and, if heavy is not NULL,
+ * the sample's heavy keys (heavy->n_heavy, heavy->heavy_keys).  The
+ * workspace is that of the default plan.  SYNCHRONISES. */
+pj_status pj_plan_features(const pj_join_desc* desc, void* workspace, size_t workspace_bytes, float* features,
+                           pj_plan* heavy, pj_stream stream);
+
+/* Candidate schedule c (0 .. PJ_PLAN_CANDIDATES-1) from the sizes and a heavy
+ * set (from pj_plan_features; NULL: none).  PJ_ERR_INVALID if c cannot be
+ * built for this join. */
+pj_status pj_plan_candidate(const pj_join_desc* desc, int32_t candidate, const pj_plan* heavy, pj_plan* plan);
+
+/* Learned plan: features, the MLP (params: device, PJ_MLP_FEATURES ->
+ * PJ_MLP_HIDDEN -> PJ_MLP_HIDDEN -> PJ_PLAN_CANDIDATES, outputs = predicted
+ * log2 milliseconds), and the best-ranked candidate that can be built.
+ * scores (host, PJ_PLAN_CANDIDATES floats, optional) receives the network's
+ * outputs.  SYNCHRONISES. */
+pj_status pj_plan_learned(const pj_join_desc* desc, const float* params, void* workspace, size_t workspace_bytes,
+                          pj_plan* plan, float* scores, pj_stream stream);
+
 /* Seeded input tables generated on the device: the reference's
  * generate_input_tables (generate_input_tables.cuh:143-226) and its Zipf
  * generator (generate_zipf_input.cuh:50-134).  Build keys lie in

@@ -65,6 +65,13 @@ class BatchConfig(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class MlpDims(ctypes.Structure):
+    _fields_ = [("in_", ctypes.c_int32), ("h1", ctypes.c_int32), ("h2", ctypes.c_int32), ("out", ctypes.c_int32)]
+
+
+MLP_FEATURES, MLP_HIDDEN, PLAN_CANDIDATES = 32, 64, 12  # PJ_MLP_FEATURES, PJ_MLP_HIDDEN, PJ_PLAN_CANDIDATES
+
+
 # every symbol include/pj.h declares, with its ctypes signature
 _P, _I32, _I64, _SZ = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
 SIGNATURES = {
@@ -96,6 +103,17 @@ SIGNATURES = {
     "pj_batch_check": (ctypes.c_int, [_P, _P]),
     "pj_batch_autotune": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Output), _I32, _P, _SZ, _P,
                                          ctypes.POINTER(BatchConfig), ctypes.POINTER(ctypes.c_float)]),
+    "pj_mlp_param_count": (ctypes.c_int64, [ctypes.POINTER(MlpDims)]),
+    "pj_mlp_forward": (ctypes.c_int, [_P, ctypes.POINTER(MlpDims), _P, _I32, _P, _P, _P]),
+    "pj_mlp_backward": (ctypes.c_int, [_P, ctypes.POINTER(MlpDims), _P, _P, _P, _I32, _P, _P, _P]),
+    "pj_mlp_mse_grad": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
+    "pj_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, _I64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   ctypes.c_float, _I32, _P]),
+    "pj_plan_features": (ctypes.c_int, [ctypes.POINTER(JoinDesc), _P, _SZ, ctypes.POINTER(ctypes.c_float),
+                                        ctypes.POINTER(Plan), _P]),
+    "pj_plan_candidate": (ctypes.c_int, [ctypes.POINTER(JoinDesc), _I32, ctypes.POINTER(Plan), ctypes.POINTER(Plan)]),
+    "pj_plan_learned": (ctypes.c_int, [ctypes.POINTER(JoinDesc), _P, _P, _SZ, ctypes.POINTER(Plan),
+                                       ctypes.POINTER(ctypes.c_float), _P]),
     "pj_generate_tables": (ctypes.c_int, [_P, _I64, _P, _I64, _I32, _I64, ctypes.c_double, _I32, ctypes.c_double,
                                           ctypes.c_uint64, _P, _P]),
 }

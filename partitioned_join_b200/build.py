@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["pj_api.cu", "pj_noalloc.cu", "pj_generate.cu", "pj_batch.cu"]
+LIB_SOURCES = ["pj_api.cu", "pj_noalloc.cu", "pj_generate.cu", "pj_batch.cu", "pj_learn.cu"]
 
 
 def _deps():

@@ -1,6 +1,7 @@
 // pj_api.cu -- host side of the C ABI in include/pj.h: planning, workspace
 // layout and the stage sequence (the reference's main.cu:762-892).
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -36,6 +37,7 @@ constexpr int HEAVY_SAMPLES = 1 << 16;     // probe keys the planner samples
 constexpr int HEAVY_MIN_SAMPLES = 32;      // a heavy key holds >= 1/2048 of the sample
 constexpr int64_t HEAVY_MIN_PROBE = 1 << 20;  // smaller probe sides: no heavy-key path
 constexpr double HEAVY_MIN_SHARE = 0.5;       // share of the probe rows the heavy keys must hold
+constexpr size_t LEARN_BYTES = 4096;          // features, activations and scores of the learned planner
 
 struct DevInfo {
     int device = -1;
@@ -187,6 +189,48 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     return PJ_OK;
 }
 
+// Widest write-combining buffer (tuples) that shared memory allows at a
+// fan-out of 2^b partitions, among whole-sector groups; 0 if none fits.
+int pick_wc(int key_bytes, int b)
+{
+    for (int W : {8, 4, 2})
+        if (sector_wc(key_bytes, W) && scatter_smem(key_bytes, W, 1 << b) <= smem_limit() &&
+            (W <= 4 || b <= 8 || key_bytes == 8))
+            return W;
+    return 0;
+}
+
+// Fewest radix bits whose expected build partition fills at most 7/8 of a
+// table of cap tuples.
+int bits_for_table(int64_t n_build, int64_t cap)
+{
+    const int64_t target = std::max<int64_t>(1, cap - cap / 8);
+    return ilog2_ceil(std::max<int64_t>(1, (n_build + target - 1) / target));
+}
+
+// Heavy probe keys of a key sample: those seen at least min_count times
+// (the most frequent PJ_MAX_HEAVY of them) go to plan->heavy_keys; returns
+// the share of the sample they cover.
+double heavy_from_sample(const std::vector<int64_t>& keys, int min_count, pj_plan* plan)
+{
+    std::unordered_map<int64_t, int> freq;
+    freq.reserve(keys.size());
+    for (int64_t k : keys) ++freq[k];
+    std::vector<std::pair<int, int64_t>> heavy;
+    for (const auto& kv : freq)
+        if (kv.second >= min_count) heavy.emplace_back(kv.second, kv.first);
+    std::sort(heavy.begin(), heavy.end(), [](const auto& x, const auto& y) {
+        return x.first != y.first ? x.first > y.first : x.second < y.second;
+    });
+    plan->n_heavy = static_cast<int32_t>(std::min<size_t>(heavy.size(), PJ_MAX_HEAVY));
+    int64_t covered = 0;
+    for (int i = 0; i < plan->n_heavy; ++i) {
+        plan->heavy_keys[i] = heavy[i].second;
+        covered += heavy[i].first;
+    }
+    return keys.empty() ? 0.0 : static_cast<double>(covered) / static_cast<double>(keys.size());
+}
+
 // Resident join CTAs per SM for this plan: shared memory and threads bound it.
 int join_ctas_per_sm(int key_bytes, const pj_plan* p)
 {
@@ -213,7 +257,7 @@ struct Layout {
     int64_t max_items = 0;
     size_t status = 0, counters = 0, b_tiles = 0, p_tiles = 0, i_tiles = 0, b_tot = 0, p_tot = 0;
     size_t b_counts = 0, p_counts = 0, heavy_total = 0, heavy_items = 0, ctrl_end = 0;
-    size_t heavy_row = 0, sample = 0;
+    size_t heavy_row = 0, sample = 0, learn = 0;
     size_t b_off = 0, p_off = 0, split = 0, items = 0, item_off = 0, item_part = 0;
     size_t cta_q = 0, cta_last = 0, seg = 0, over_b = 0, over_p = 0;
     int max_ctas = 0;
@@ -272,6 +316,7 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.ctrl_end = o;
     L.heavy_row = take(4 * MAX_HEAVY);
     L.sample = take(8 * static_cast<size_t>(HEAVY_SAMPLES));
+    L.learn = take(LEARN_BYTES);
     L.b_off = take(8 * static_cast<size_t>(mb + 1));
     L.p_off = take(8 * static_cast<size_t>(mp + 1));
     L.split = take(4 * static_cast<size_t>(L.P));
@@ -343,6 +388,61 @@ __global__ void hash_slots_kernel(const K* __restrict__ keys, int64_t n, int32_t
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const uint32_t h = hash_key(keys[i]);
         out[i] = static_cast<int32_t>(ref ? slot_ref(h, T) : slot_fast(h, skip, static_cast<uint32_t>(T)));
+    }
+}
+
+// Features of the learned planner, from a sample of the probe keys (one
+// CTA): a 1024-bin sketch of the sample by hash, sorted by count, read at
+// log-spaced ranks (the shape of the key-frequency curve, whichever keys are
+// heavy), plus the sizes and the key width.  The sample keys go to
+// sample_out for the heavy-key candidates.
+constexpr int SKETCH_BINS = 1024;
+__constant__ int c_feature_ranks[20] = {0, 1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768};
+
+template <typename K>
+__global__ void __launch_bounds__(SKETCH_BINS) plan_features_kernel(const K* __restrict__ keys, int64_t n,
+                                                                   int32_t samples, int64_t* __restrict__ sample_out,
+                                                                   float* __restrict__ feat, float log_nb, float log_np,
+                                                                   float key_bytes, float unique)
+{
+    __shared__ uint32_t bins[SKETCH_BINS];
+    const int t = threadIdx.x;
+    bins[t] = 0;
+    __syncthreads();
+    for (int s = t; s < samples; s += SKETCH_BINS) {
+        const K k = keys[sample_pos(s, n)];
+        sample_out[s] = static_cast<int64_t>(k);
+        atomicAdd(&bins[hash_key(k) & (SKETCH_BINS - 1)], 1u);
+    }
+    __syncthreads();
+    // bitonic sort, descending
+    for (int size = 2; size <= SKETCH_BINS; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const int o = t ^ stride;
+            if (o > t) {
+                const uint32_t a = bins[t], b = bins[o];
+                const bool desc = (t & size) == 0;
+                if (desc ? a < b : a > b) {
+                    bins[t] = b;
+                    bins[o] = a;
+                }
+            }
+            __syncthreads();
+        }
+    const float scale = static_cast<float>(SKETCH_BINS) / static_cast<float>(samples > 0 ? samples : 1);
+    if (t < 20) feat[t] = log2f(1.0f + bins[c_feature_ranks[t]] * scale);
+    if (t == 0) {
+        uint32_t top = 0, nonempty = 0;
+        for (int i = 0; i < 16; ++i) top += bins[i];
+        for (int i = 0; i < SKETCH_BINS; ++i) nonempty += bins[i] ? 1u : 0u;
+        feat[20] = static_cast<float>(top) / static_cast<float>(samples > 0 ? samples : 1);
+        feat[21] = static_cast<float>(nonempty) / SKETCH_BINS;
+        feat[22] = log_nb / 32.0f;
+        feat[23] = log_np / 32.0f;
+        feat[24] = (log_np - log_nb) / 8.0f;
+        feat[25] = key_bytes / 8.0f;
+        feat[26] = unique;
+        for (int i = 27; i < PJ_MLP_FEATURES; ++i) feat[i] = 0.0f;
     }
 }
 
@@ -767,19 +867,8 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     }
     p->scatter_ctas_per_sm = 1;
     p->hist_split = 2;
-    // Widest write-combining buffer that the shared memory allows at a fan-out.
-    auto pick_w = [&](int b) {
-        for (int W : {8, 4, 2})
-            if (sector_wc(d->key_bytes, W) && scatter_smem(d->key_bytes, W, 1 << b) <= smem_limit() &&
-                (W <= 4 || b <= 8 || d->key_bytes == 8))
-                return W;
-        return 0;
-    };
-    // Fewest partitions whose expected build side fills at most 7/8 of a table.
-    auto bits_for = [&](int64_t cap) {
-        const int64_t target = std::max<int64_t>(1, cap - cap / 8);
-        return ilog2_ceil(std::max<int64_t>(1, (d->n_build + target - 1) / target));
-    };
+    auto pick_w = [&](int b) { return pick_wc(d->key_bytes, b); };
+    auto bits_for = [&](int64_t cap) { return bits_for_table(d->n_build, cap); };
     int bits = bits_for(p->table_capacity);
     if (pick_w(bits) == 0) {
         // beyond one pass's fan-out: 4-byte COMPACT entries hold twice the
@@ -1050,26 +1139,10 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
         return PJ_ERR_CUDA;
     }
     if (sample) {
-        // heavy: at least HEAVY_MIN_SAMPLES of the sample (>= 1/2048 of the
-        // probe rows); the most frequent PJ_MAX_HEAVY of them
-        std::unordered_map<int64_t, int> freq;
-        freq.reserve(keys_h.size());
-        for (int64_t k : keys_h) ++freq[k];
-        std::vector<std::pair<int, int64_t>> heavy;
-        for (const auto& kv : freq)
-            if (kv.second >= HEAVY_MIN_SAMPLES) heavy.emplace_back(kv.second, kv.first);
-        std::sort(heavy.begin(), heavy.end(), [](const auto& x, const auto& y) {
-            return x.first != y.first ? x.first > y.first : x.second < y.second;
-        });
-        p.n_heavy = static_cast<int32_t>(std::min<size_t>(heavy.size(), PJ_MAX_HEAVY));
-        int64_t covered = 0;
-        for (int i = 0; i < p.n_heavy; ++i) {
-            p.heavy_keys[i] = heavy[i].second;
-            covered += heavy[i].first;
-        }
         // the path pays a lookup for every probe key: worth it only when the
         // heavy keys carry a large share of the probe side
-        if (covered < static_cast<int64_t>(HEAVY_MIN_SHARE * HEAVY_SAMPLES)) p.n_heavy = 0;
+        const double share = heavy_from_sample(keys_h, HEAVY_MIN_SAMPLES, &p);
+        if (share < HEAVY_MIN_SHARE) p.n_heavy = 0;
     }
     int64_t raw_max = 0, hash_max = 0;
     for (int i = 0; i < P; ++i) {
@@ -1092,6 +1165,107 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
     if (mx > cap * (int64_t(1) << MAX_SPLIT_LOG2) / 2) p.split_mode = PJ_SPLIT_POSITION;
     *plan = p;
     return PJ_OK;
+}
+
+// ---- learned planner ------------------------------------------------------
+
+pj_status pj_plan_features(const pj_join_desc* d, void* ws, size_t ws_bytes, float* features, pj_plan* heavy,
+                           pj_stream stream)
+{
+    if (!valid_desc(d) || !features) return PJ_ERR_INVALID;
+    pj_plan p;
+    pj_status s = pj_plan_default(d, &p);
+    if (s != PJ_OK) return s;
+    Layout L;
+    if ((s = check_ws(d, &p, ws, ws_bytes, &L)) != PJ_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    float* feat_d = reinterpret_cast<float*>(w + L.learn);
+    int64_t* sample_d = reinterpret_cast<int64_t*>(w + L.sample);
+    const int samples = d->n_probe > 0 ? static_cast<int>(std::min<int64_t>(std::max<int64_t>(d->n_probe / 100, 4096),
+                                                                            HEAVY_SAMPLES))
+                                       : 0;
+    const float lnb = static_cast<float>(std::log2(static_cast<double>(std::max<int64_t>(d->n_build, 1))));
+    const float lnp = static_cast<float>(std::log2(static_cast<double>(std::max<int64_t>(d->n_probe, 1))));
+    if (samples > 0 && !aligned16(d->probe_keys)) return PJ_ERR_ALIGNMENT;
+    if (d->key_bytes == 4)
+        plan_features_kernel<int32_t><<<1, SKETCH_BINS, 0, st>>>(static_cast<const int32_t*>(d->probe_keys), d->n_probe,
+                                                                 samples, sample_d, feat_d, lnb, lnp, 4.0f,
+                                                                 d->unique_build_keys ? 1.0f : 0.0f);
+    else
+        plan_features_kernel<int64_t><<<1, SKETCH_BINS, 0, st>>>(static_cast<const int64_t*>(d->probe_keys), d->n_probe,
+                                                                 samples, sample_d, feat_d, lnb, lnp, 8.0f,
+                                                                 d->unique_build_keys ? 1.0f : 0.0f);
+    PJ_CUDA(cudaGetLastError());
+    std::vector<int64_t> keys_h(static_cast<size_t>(heavy ? samples : 0));
+    PJ_CUDA(cudaMemcpyAsync(features, feat_d, sizeof(float) * PJ_MLP_FEATURES, cudaMemcpyDeviceToHost, st));
+    if (heavy && samples > 0)
+        PJ_CUDA(cudaMemcpyAsync(keys_h.data(), sample_d, sizeof(int64_t) * samples, cudaMemcpyDeviceToHost, st));
+    PJ_CUDA(cudaStreamSynchronize(st));
+    if (heavy) {
+        std::memset(heavy, 0, sizeof(*heavy));
+        if (d->unique_build_keys && samples > 0)
+            heavy_from_sample(keys_h, std::max(2, samples / 2048), heavy);
+    }
+    return PJ_OK;
+}
+
+pj_status pj_plan_candidate(const pj_join_desc* d, int32_t candidate, const pj_plan* heavy, pj_plan* plan)
+{
+    if (!valid_desc(d) || !plan || candidate < 0 || candidate >= PJ_PLAN_CANDIDATES) return PJ_ERR_INVALID;
+    pj_plan p;
+    pj_status s = pj_plan_default(d, &p);
+    if (s != PJ_OK) return s;
+    const int table = candidate / 6, delta = (candidate % 6) / 2 - 1, heavy_on = candidate % 2;
+    p.table_mode = table ? PJ_TABLE_COMPACT : PJ_TABLE_BUCKET;
+    p.table_capacity = max_table_capacity(d->key_bytes, p.table_mode);
+    int max_bits = 0;
+    for (int b = 0; b <= 16; ++b)
+        if (pick_wc(d->key_bytes, b) != 0) max_bits = b;
+    const int bits = std::min(std::max(bits_for_table(d->n_build, p.table_capacity) + delta, 0), max_bits);
+    p.bits1 = bits;
+    p.wc_tuples = pick_wc(d->key_bytes, bits);
+    if (p.wc_tuples == 0) return PJ_ERR_INVALID;
+    p.n_heavy = 0;
+    if (heavy_on && heavy && d->unique_build_keys && heavy->n_heavy > 0) {
+        p.n_heavy = std::min(heavy->n_heavy, PJ_MAX_HEAVY);
+        for (int i = 0; i < p.n_heavy; ++i) p.heavy_keys[i] = heavy->heavy_keys[i];
+    }
+    if ((s = check_plan(d, &p)) != PJ_OK) return s;
+    *plan = p;
+    return PJ_OK;
+}
+
+pj_status pj_plan_learned(const pj_join_desc* d, const float* params, void* ws, size_t ws_bytes, pj_plan* plan,
+                          float* scores, pj_stream stream)
+{
+    if (!valid_desc(d) || !plan || !params) return PJ_ERR_INVALID;
+    float feat[PJ_MLP_FEATURES];
+    pj_plan heavy;
+    pj_status s = pj_plan_features(d, ws, ws_bytes, feat, &heavy, stream);
+    if (s != PJ_OK) return s;
+    pj_plan p0;
+    pj_plan_default(d, &p0);
+    Layout L;
+    if ((s = check_ws(d, &p0, ws, ws_bytes, &L)) != PJ_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    float* feat_d = reinterpret_cast<float*>(static_cast<uint8_t*>(ws) + L.learn);
+    const pj_mlp_dims dims{PJ_MLP_FEATURES, PJ_MLP_HIDDEN, PJ_MLP_HIDDEN, PJ_PLAN_CANDIDATES};
+    float* acts_d = feat_d + PJ_MLP_FEATURES;
+    float* out_d = acts_d + 4 * PJ_MLP_HIDDEN;
+    static_assert((PJ_MLP_FEATURES + 4 * PJ_MLP_HIDDEN + PJ_PLAN_CANDIDATES) * sizeof(float) <= LEARN_BYTES,
+                  "learned-planner scratch");
+    if ((s = pj_mlp_forward(params, &dims, feat_d, 1, acts_d, out_d, stream)) != PJ_OK) return s;
+    float out[PJ_PLAN_CANDIDATES];
+    PJ_CUDA(cudaMemcpyAsync(out, out_d, sizeof(out), cudaMemcpyDeviceToHost, st));
+    PJ_CUDA(cudaStreamSynchronize(st));
+    if (scores) std::memcpy(scores, out, sizeof(out));
+    int order[PJ_PLAN_CANDIDATES];
+    for (int i = 0; i < PJ_PLAN_CANDIDATES; ++i) order[i] = i;
+    std::sort(order, order + PJ_PLAN_CANDIDATES, [&](int a, int b) { return out[a] < out[b]; });
+    for (int c : order)
+        if (pj_plan_candidate(d, c, &heavy, plan) == PJ_OK) return PJ_OK;
+    return pj_plan_default(d, plan);
 }
 
 }  // extern "C"

@@ -125,22 +125,27 @@ __global__ void __launch_bounds__(512) heavy_rows_kernel(const K* __restrict__ k
     }
 }
 
+// Position of sample s in a column of n rows (SplitMix64 of s).
+__device__ __forceinline__ int64_t sample_pos(int s, int64_t n)
+{
+    uint64_t x = static_cast<uint64_t>(s) * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return static_cast<int64_t>(x % static_cast<uint64_t>(n));
+}
+
 // Keys at pseudo-random positions of a column (the planner's sample).
 template <typename K>
 __global__ void sample_keys_kernel(const K* __restrict__ keys, int64_t n, int32_t samples, int64_t* __restrict__ out)
 {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < samples; s += gridDim.x * blockDim.x) {
-        uint64_t x = static_cast<uint64_t>(s) * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull;
-        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
-        x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
-        x ^= x >> 31;
-        out[s] = static_cast<int64_t>(keys[x % static_cast<uint64_t>(n)]);
-    }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < samples; s += gridDim.x * blockDim.x)
+        out[s] = static_cast<int64_t>(keys[sample_pos(s, n)]);
 }
 
 // H = the heavy pairs of every item: the output count so far, where the
 // join's output chunks begin.  One warp.
-__global__ void heavy_total_kernel(const unsigned long long* __restrict__ item_count, int32_t n_items,
+static __global__ void heavy_total_kernel(const unsigned long long* __restrict__ item_count, int32_t n_items,
                                    unsigned long long* __restrict__ total, unsigned long long* __restrict__ count)
 {
     unsigned long long sum = 0;
