@@ -46,9 +46,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["cfg2", "cfg3", "cfg5"], default="cfg2",
+    ap.add_argument("--workload", choices=["cfg2", "cfg3", "cfg4", "cfg5"], default="cfg2",
                     help="cfg2: 2^27 x 2^27 int32 uniform (the headline); cfg3: 2^26 x 2^28 int64, Zipf probe "
-                         "keys; cfg5: 512 int32 joins of uneven sizes, batched against one after another")
+                         "keys; cfg4: learned against exact plans on a held-out sweep; cfg5: 512 int32 joins of "
+                         "uneven sizes, batched against one after another")
+    ap.add_argument("--sweep", type=int, default=80, help="cfg4: held-out workloads")
     ap.add_argument("--batch", type=int, default=512, help="cfg5: joins in the batch")
     ap.add_argument("--zipf", type=float, default=1.0, help="cfg3: Zipf exponent of the probe keys")
     ap.add_argument("--log2-build", type=int, default=None)
@@ -488,6 +490,82 @@ def run_batch(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_learned(args, rank, world, local):
+    """cfg4: the shipped planner weights against the exact-histogram planner
+    on a held-out seeded sweep (build 2^14..2^24 log-uniform, probe/build 1,
+    4 or 16, int32 or int64, Zipf 0..1.5, match rate 0.1..1).  Per workload
+    both plans are made and timed (join time, and planning time apart);
+    value = geometric-mean speedup of the learned plans' joins, fallbacks
+    (a learned plan that overflows, rerun with the exact plan) counted at
+    their full cost."""
+    import numpy as np
+    import torch
+
+    from partitioned_join_b200 import _lib, api, planner
+
+    torch.cuda.set_device(local)
+    params = planner.load_weights(device=torch.device("cuda", local))
+    if params is None:
+        raise SystemExit("no planner weights (partitioned_join_b200/planner_weights.npz)")
+    rng = np.random.default_rng(args.seed + 424242)
+    rows = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def time_join(b, p, plan):
+        j = api.Joiner(b, p, True, plan)
+        j.launch()
+        st = j.status()
+        best = float("inf")
+        for _ in range(2):
+            e0.record()
+            j.launch()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best, st
+
+    for i in range(args.sweep):
+        b, p, meta = planner.sweep_workload(rng, 24, 26)
+        t0 = time.perf_counter()
+        exact = api.plan_exact(b, p, True)
+        plan_exact_ms = 1e3 * (time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        learned, _ = planner.plan_learned(b, p, True, params)
+        plan_learned_ms = 1e3 * (time.perf_counter() - t0)
+        t_exact, st = time_join(b, p, exact)
+        _lib.check(st, "exact plan")
+        t_learned, st = time_join(b, p, learned)
+        fallback = st != _lib.OK
+        if fallback:
+            t_learned += t_exact
+        rows.append(dict(meta, t_exact=t_exact, t_learned=t_learned, fallback=fallback, plan_exact_ms=plan_exact_ms,
+                         plan_learned_ms=plan_learned_ms))
+        del b, p
+    sp = np.array([r["t_exact"] / r["t_learned"] for r in rows])
+    z = np.array([r["zipf"] for r in rows])
+    geo = float(np.exp(np.log(sp).mean()))
+
+    def geo_of(mask):
+        return float(np.exp(np.log(sp[mask]).mean())) if mask.any() else None
+
+    line = {
+        "metric": "geomean speedup of learned over exact plans (cfg4 held-out sweep)", "value": geo, "unit": "x",
+        "n_gpus": world, "steps": 2, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/int64", "data": "synthetic",
+        "config": {"workload": f"{args.sweep} held-out joins: build 2^14..2^24 log-uniform, probe/build 1/4/16, "
+                               "int32 or int64, Zipf 0..1.5, match 0.1..1 (generated on the device)"},
+        "fallback_rate": float(np.mean([r["fallback"] for r in rows])),
+        "speedup_by_zipf": {"uniform(<0.2)": geo_of(z < 0.2), "0.2-1.0": geo_of((z >= 0.2) & (z < 1.0)),
+                            ">=1.0": geo_of(z >= 1.0)},
+        "join_ms_total": {"exact": float(sum(r["t_exact"] for r in rows)),
+                          "learned": float(sum(r["t_learned"] for r in rows))},
+        "planning_ms_median": {"exact": float(np.median([r["plan_exact_ms"] for r in rows])),
+                               "learned": float(np.median([r["plan_learned_ms"] for r in rows]))},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
@@ -495,6 +573,8 @@ def main():
         run_reference(args, rank, world)
     elif args.workload == "cfg5":
         run_batch(args, rank, world, local)
+    elif args.workload == "cfg4":
+        run_learned(args, rank, world, local)
     else:
         run_ours(args, rank, world, local)
 
