@@ -115,16 +115,21 @@ enum {
  * pj_plan_exact() from device histograms.  Passing NULL to pj_inner_join()
  * uses pj_plan_default(). */
 typedef struct pj_plan {
-    int32_t passes;             /* radix passes (1) */
+    int32_t passes;             /* radix passes: 1, or 2 (pass 2 splits each pass-1
+                                   partition by the next bits2 digit bits, as the
+                                   reference's partition_input_tables_pass_two,
+                                   partitioned_join.cuh:109-175) */
     int32_t bits1;              /* radix bits of pass 1: 2^bits1 partitions */
-    int32_t bits2;              /* radix bits of pass 2 (0) */
+    int32_t bits2;              /* radix bits of pass 2 (0 for one pass); the join
+                                   sees 2^(bits1+bits2) partitions */
     int32_t digit_mode;         /* PJ_DIGIT_* */
     int32_t table_mode;         /* PJ_TABLE_* */
     int32_t slot_mode;          /* PJ_SLOT_* (PJ_TABLE_OPEN) */
     int32_t split_mode;         /* PJ_SPLIT_* */
     int32_t table_capacity;     /* BUCKET: build tuples one table holds; OPEN: slots */
     int32_t probe_chunk;        /* probe tuples of one join work item (multiple of 16) */
-    int32_t wc_tuples;          /* tuples per write-combining buffer: 2, 4 or 8 */
+    int32_t wc_tuples;          /* tuples per write-combining buffer of pass 1:
+                                   2, 4, 8, 16 or 32 (pass 2 sizes its own) */
     int32_t scatter_ctas_per_sm;/* scatter chunks per SM */
     int32_t hist_split;         /* histogram CTAs per scatter chunk */
     float max_fill;             /* OPEN: target fill (the reference's HASH_TABLE_OCC = 0.5) */

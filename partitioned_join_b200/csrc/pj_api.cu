@@ -103,14 +103,30 @@ constexpr int sc_v() { return sizeof(K) == 4 ? SC_V32 : SC_V64; }
 
 int tuple_words(int key_bytes) { return key_bytes == 4 ? 2 : 4; }
 
-size_t scatter_smem(int key_bytes, int W, int P)
+// Shared memory of the scatter with P buffers of cap tuples each.
+size_t scatter_smem(int key_bytes, int cap, int P)
 {
-    return static_cast<size_t>(P) * W * tuple_words(key_bytes) * 4 + static_cast<size_t>(P) * 8;
+    return static_cast<size_t>(P) * cap * tuple_words(key_bytes) * 4 + static_cast<size_t>(P) * 8;
+}
+
+// Tuples per partition buffer of a scatter whose rounds bring `round` tuples
+// over P partitions, in groups of W: a round's expected arrivals per
+// partition plus three standard deviations and one partial group, so that
+// nearly every group completes inside the buffer and leaves as whole
+// sectors; at most what shared memory holds beside `extra` bytes, at least W.
+int wc_cap(int key_bytes, int W, int P, int round, size_t extra)
+{
+    const double m = static_cast<double>(round) / P;
+    int want = static_cast<int>(std::ceil(m + 3.0 * std::sqrt(m))) + W;
+    want = (want + W - 1) / W * W;
+    const size_t room = smem_limit() > extra + static_cast<size_t>(P) * 8 ? smem_limit() - extra - static_cast<size_t>(P) * 8 : 0;
+    const int fit = static_cast<int>(std::min<size_t>(room / (static_cast<size_t>(P) * tuple_words(key_bytes) * 4), 1 << 20)) / W * W;
+    return std::max(W, std::min(want, fit));
 }
 
 bool valid_wc(int key_bytes, int W)
 {
-    if (W != 2 && W != 4 && W != 8) return false;
+    if (W != 2 && W != 4 && W != 8 && W != 16 && W != 32) return false;
     return (W * tuple_words(key_bytes) * 4) % 16 == 0;
 }
 
@@ -162,9 +178,14 @@ bool valid_desc(const pj_join_desc* d)
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+int pass2_wc(int key_bytes, const pj_plan* p);
+
 pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
 {
-    if (p->passes != 1 || p->bits2 != 0) return PJ_ERR_INVALID;
+    if (p->passes != 1 && p->passes != 2) return PJ_ERR_INVALID;
+    if (p->passes == 1 ? p->bits2 != 0 : (p->bits1 < 1 || p->bits2 < 1 || p->bits1 + p->bits2 > 22))
+        return PJ_ERR_INVALID;
+    if (p->passes == 2 && pass2_wc(d->key_bytes, p) == 0) return PJ_ERR_INVALID;
     if (p->bits1 < 0 || p->bits1 > 16) return PJ_ERR_INVALID;
     if (!valid_wc(d->key_bytes, p->wc_tuples)) return PJ_ERR_INVALID;
     if (scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) > smem_limit()) return PJ_ERR_INVALID;
@@ -183,22 +204,26 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (p->n_heavy > 0 && scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) + HeavyTable::BYTES + 16 > smem_limit())
         return PJ_ERR_INVALID;  // the probe scatter also holds the heavy table
     // hash bits: digits + hash split + bucket/slot bits must fit 32
-    const int digit_bits = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0;
+    const int digit_bits = (p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0) + (p->passes == 2 ? p->bits2 : 0);
     const int slot_bits = p->table_mode != PJ_TABLE_OPEN ? bucket_nb_log2(p->table_capacity) : 12;
-    if (digit_bits + MAX_SPLIT_LOG2 + slot_bits > 32) return PJ_ERR_INVALID;
+    // digits and bucket bits disjoint; the bits of a hash split (below the
+    // digits) may overlap the bucket bits: pieces stay exact, buckets coarser
+    if (digit_bits + slot_bits > 32 || digit_bits + MAX_SPLIT_LOG2 > 31) return PJ_ERR_INVALID;
     return PJ_OK;
 }
 
-// Widest write-combining buffer (tuples) that shared memory allows at a
-// fan-out of 2^b partitions, among whole-sector groups; 0 if none fits.
+// Write-combining group (tuples): the smallest whole-sector group whose
+// buffers fit shared memory at a fan-out of 2^b partitions; 0 if none fits.
+// Where the fan-out is low the buffers hold several groups (wc_cap).
 int pick_wc(int key_bytes, int b)
 {
-    for (int W : {8, 4, 2})
-        if (sector_wc(key_bytes, W) && scatter_smem(key_bytes, W, 1 << b) <= smem_limit() &&
-            (W <= 4 || b <= 8 || key_bytes == 8))
-            return W;
+    for (int W : {2, 4, 8, 16, 32})
+        if (sector_wc(key_bytes, W) && scatter_smem(key_bytes, W, 1 << b) <= smem_limit()) return W;
     return 0;
 }
+
+// Write-combining width of a two-pass plan's second pass (its own fan-out).
+int pass2_wc(int key_bytes, const pj_plan* p) { return pick_wc(key_bytes, p->bits2); }
 
 // Fewest radix bits whose expected build partition fills at most 7/8 of a
 // table of cap tuples.
@@ -250,7 +275,13 @@ int table_tuples(const pj_plan* p)
 // ---------------------------------------------------------------------------
 // Workspace layout.  Everything 256-byte aligned.
 struct Layout {
-    int P = 1;
+    int P = 1;    // partitions the join sees (P1 * P2 for two-pass plans)
+    int P1 = 1;   // partitions of the first pass
+    int C = 0;    // two-pass plans: slices per first-pass partition in the second pass
+    int64_t b_cap2 = 0, p_cap2 = 0;  // tuples of the second pass's output
+    size_t b_tiles2 = 0, p_tiles2 = 0, b_counts2 = 0, p_counts2 = 0, b_off2 = 0, p_off2 = 0;
+    size_t b_tuples2 = 0, p_tuples2 = 0;
+    int64_t b_tiles2_n = 0, p_tiles2_n = 0;
     int b_items = 1, p_items = 1;
     int64_t b_chunk = 16, p_chunk = 16;
     int64_t b_cap = 0, p_cap = 0;  // tuples
@@ -266,7 +297,7 @@ struct Layout {
     int64_t b_tiles_n = 0, p_tiles_n = 0, i_tiles_n = 0;
 };
 
-constexpr int CTR_QUEUE = 0, CTR_BTILE = 1, CTR_PTILE = 2, CTR_ITILE = 3;
+constexpr int CTR_QUEUE = 0, CTR_BTILE = 1, CTR_PTILE = 2, CTR_ITILE = 3, CTR_BTILE2 = 4, CTR_PTILE2 = 5;
 
 int64_t chunk_for(int64_t n, int items)
 {
@@ -282,13 +313,24 @@ int64_t part_capacity(int64_t n, int P, int items, int W) { return n + static_ca
 Layout make_layout(const pj_join_desc* d, const pj_plan* p)
 {
     Layout L;
-    L.P = 1 << p->bits1;
+    const bool two = p->passes == 2;
+    L.P1 = 1 << p->bits1;
+    L.P = two ? L.P1 << p->bits2 : L.P1;
     L.b_items = L.p_items = scatter_items(p);
     L.b_chunk = chunk_for(d->n_build, L.b_items);
     L.p_chunk = chunk_for(d->n_probe, L.p_items);
-    L.b_cap = part_capacity(d->n_build, L.P, L.b_items, p->wc_tuples);
-    L.p_cap = part_capacity(d->n_probe, L.P, L.p_items, p->wc_tuples);
-    const int64_t mb = static_cast<int64_t>(L.P) * L.b_items, mp = static_cast<int64_t>(L.P) * L.p_items;
+    L.b_cap = part_capacity(d->n_build, L.P1, L.b_items, p->wc_tuples);
+    L.p_cap = part_capacity(d->n_probe, L.P1, L.p_items, p->wc_tuples);
+    if (two) {
+        // second pass: about four items per SM over the first pass's
+        // partitions (items of one partition's slices are near-equal)
+        L.C = std::max(1, (4 * sm_count() + L.P1 - 1) / L.P1);
+        L.b_cap2 = part_capacity(d->n_build, L.P, L.C, pass2_wc(d->key_bytes, p));
+        L.p_cap2 = part_capacity(d->n_probe, L.P, L.C, pass2_wc(d->key_bytes, p));
+    }
+    const int64_t m2 = static_cast<int64_t>(L.P) * L.C;  // second-pass segments per side
+    L.b_tiles2_n = L.p_tiles2_n = two ? (m2 + SCAN_TILE - 1) / SCAN_TILE + 1 : 0;
+    const int64_t mb = static_cast<int64_t>(L.P1) * L.b_items, mp = static_cast<int64_t>(L.P1) * L.p_items;
     L.b_tiles_n = (mb + SCAN_TILE - 1) / SCAN_TILE + 1;
     L.p_tiles_n = (mp + SCAN_TILE - 1) / SCAN_TILE + 1;
     L.i_tiles_n = (L.P + SCAN_TILE - 1) / SCAN_TILE + 1;
@@ -313,6 +355,12 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.p_counts = take(4 * static_cast<size_t>(mp));
     L.heavy_total = take(8);
     L.heavy_items = take(8 * static_cast<size_t>(L.p_items));
+    if (two) {
+        L.b_tiles2 = take(8 * L.b_tiles2_n);
+        L.p_tiles2 = take(8 * L.p_tiles2_n);
+        L.b_counts2 = take(4 * static_cast<size_t>(m2));
+        L.p_counts2 = take(4 * static_cast<size_t>(m2));
+    }
     L.ctrl_end = o;
     L.heavy_row = take(4 * MAX_HEAVY);
     L.sample = take(8 * static_cast<size_t>(HEAVY_SAMPLES));
@@ -335,6 +383,12 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     const int TW = tuple_words(d->key_bytes);
     L.b_tuples = take(4 * static_cast<size_t>(TW) * L.b_cap + 64);
     L.p_tuples = take(4 * static_cast<size_t>(TW) * L.p_cap + 64);
+    if (two) {
+        L.b_off2 = take(8 * static_cast<size_t>(m2 + 1));
+        L.p_off2 = take(8 * static_cast<size_t>(m2 + 1));
+        L.b_tuples2 = take(4 * static_cast<size_t>(TW) * L.b_cap2 + 64);
+        L.p_tuples2 = take(4 * static_cast<size_t>(TW) * L.p_cap2 + 64);
+    }
     L.total = o;
     return L;
 }
@@ -531,12 +585,13 @@ pj_status launch_scatter_t(const K* keys, int64_t n, int64_t chunk, int items, D
                            const HeavyCtx& hc, cudaStream_t st)
 {
     auto* kern = scatter_keys_kernel<K, SC_THREADS, sc_v<K>(), W, HASHD, HEAVY>;
-    const size_t smem = HEAVY ? heavy_table_offset(P, WcTraits<K, W>::BW) + HeavyTable::BYTES
-                              : scatter_smem(sizeof(K), W, P);
+    constexpr int TW = WcTraits<K, W>::TW;
+    const int cap = wc_cap(sizeof(K), W, P, SC_THREADS * sc_v<K>(), HEAVY ? HeavyTable::BYTES + 16 : 0);
+    const size_t smem = HEAVY ? heavy_table_offset(P, cap * TW) + HeavyTable::BYTES : scatter_smem(sizeof(K), cap, P);
     PJ_CUDA(set_smem(kern, smem));
     typename HeavyArg<HEAVY>::type h{};
     if constexpr (HEAVY) h = *hc.hs;
-    kern<<<items, SC_THREADS, smem, st>>>(keys, n, chunk, items, f, P, offsets, out,
+    kern<<<items, SC_THREADS, smem, st>>>(keys, n, chunk, items, f, P, cap, offsets, out,
                                          static_cast<uint32_t>(std::min<int64_t>(out_cap, UINT32_MAX)), status, h,
                                          hc.out);
     PJ_CUDA(cudaGetLastError());
@@ -564,6 +619,8 @@ pj_status launch_scatter(const K* keys, int64_t n, int64_t chunk, int items, Dig
     if (W == 2) return launch_scatter_w<K, 2>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
     if (W == 4) return launch_scatter_w<K, 4>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
     if (W == 8) return launch_scatter_w<K, 8>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
+    if (W == 16) return launch_scatter_w<K, 16>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
+    if (W == 32) return launch_scatter_w<K, 32>(keys, n, chunk, items, f, P, offsets, out, out_cap, status, hc, st);
     return PJ_ERR_INVALID;
 }
 
@@ -632,23 +689,82 @@ pj_status partition_column(const K* keys, int64_t n, const pj_plan* p, const Lay
                            const HeavyCtx& hc = HeavyCtx())
 {
     const DigitFn f = digit_fn(p->digit_mode, 0, p->bits1, 0);
+    const int P1 = L.P1;
     const int64_t chunk = side == 0 ? L.b_chunk : L.p_chunk;
     const int items = side == 0 ? L.b_items : L.p_items;
     uint32_t* status = reinterpret_cast<uint32_t*>(ws + L.status);
     uint32_t* ctr = reinterpret_cast<uint32_t*>(ws + L.counters);
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + (side == 0 ? L.b_counts : L.p_counts));
-    int32_t* tot = reinterpret_cast<int32_t*>(ws + (side == 0 ? L.b_tot : L.p_tot));
+    // per-partition totals feed the join's work split: the second pass
+    // writes them for two-pass plans
+    int32_t* tot = p->passes == 2 ? nullptr : reinterpret_cast<int32_t*>(ws + (side == 0 ? L.b_tot : L.p_tot));
     int64_t* off = reinterpret_cast<int64_t*>(ws + (side == 0 ? L.b_off : L.p_off));
     uint64_t* tiles = reinterpret_cast<uint64_t*>(ws + (side == 0 ? L.b_tiles : L.p_tiles));
     pj_status s;
     E.mark(stage0, st);
-    if ((s = launch_hist<K>(keys, n, chunk, items, p->hist_split, f, L.P, counts, tot, st, hc)) != PJ_OK) return s;
+    if ((s = launch_hist<K>(keys, n, chunk, items, p->hist_split, f, P1, counts, tot, st, hc)) != PJ_OK) return s;
     E.mark(stage0 + 1, st);
-    if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(L.P) * items, static_cast<uint32_t>(p->wc_tuples), off,
+    if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(P1) * items, static_cast<uint32_t>(p->wc_tuples), off,
                                    tiles, ctr + (side == 0 ? CTR_BTILE : CTR_PTILE), status, st)) != PJ_OK)
         return s;
     E.mark(stage0 + 2, st);
-    return launch_scatter<K>(keys, n, chunk, items, f, L.P, p->wc_tuples, off, tuples, cap, status, st, hc);
+    return launch_scatter<K>(keys, n, chunk, items, f, P1, p->wc_tuples, off, tuples, cap, status, st, hc);
+}
+
+// Second pass of a two-pass plan over one side's first-pass tuples:
+// histogram -> look-back scan -> scatter into the side's second tuple buffer.
+// The digit is the next bits2 hash bits below those the first pass used.
+template <typename K, int W>
+pj_status launch_scatter_tuples(const uint32_t* in, const Pass2Items& it, int n_items, DigitFn f, int P2,
+                                const int64_t* off, uint32_t* out, int64_t cap, uint32_t* status, cudaStream_t st)
+{
+    constexpr int VT = sizeof(K) == 4 ? 4 : 2;
+    auto* kern = scatter_tuples_kernel<K, SC_THREADS, VT, W>;
+    const int bcap = wc_cap(sizeof(K), W, P2, SC_THREADS * VT, 0);
+    const size_t smem = scatter_smem(sizeof(K), bcap, P2);
+    PJ_CUDA(set_smem(kern, smem));
+    const int grid = std::min(n_items, sm_count());
+    kern<<<grid, SC_THREADS, smem, st>>>(in, it, n_items, f, P2, bcap, off,
+                                        out, static_cast<uint32_t>(std::min<int64_t>(cap, UINT32_MAX)), status);
+    PJ_CUDA(cudaGetLastError());
+    return PJ_OK;
+}
+
+template <typename K>
+pj_status partition_pass2(const pj_plan* p, const Layout& L, int side, uint8_t* ws, uint32_t* out, int64_t cap,
+                          cudaStream_t st)
+{
+    const int hb = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0;  // hash bits the first pass used
+    const DigitFn f = digit_fn(PJ_DIGIT_HASH, hb, p->bits2, 0);
+    const int P2 = 1 << p->bits2;
+    const int items1 = side == 0 ? L.b_items : L.p_items;
+    const int n_items = L.P1 * L.C;
+    uint32_t* status = reinterpret_cast<uint32_t*>(ws + L.status);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(ws + L.counters);
+    const Pass2Items it{reinterpret_cast<const int64_t*>(ws + (side == 0 ? L.b_off : L.p_off)), items1, L.C};
+    const uint32_t* in = reinterpret_cast<const uint32_t*>(ws + (side == 0 ? L.b_tuples : L.p_tuples));
+    uint32_t* counts = reinterpret_cast<uint32_t*>(ws + (side == 0 ? L.b_counts2 : L.p_counts2));
+    int32_t* tot = reinterpret_cast<int32_t*>(ws + (side == 0 ? L.b_tot : L.p_tot));
+    int64_t* off = reinterpret_cast<int64_t*>(ws + (side == 0 ? L.b_off2 : L.p_off2));
+    uint64_t* tiles = reinterpret_cast<uint64_t*>(ws + (side == 0 ? L.b_tiles2 : L.p_tiles2));
+    const size_t hsmem = 4 * static_cast<size_t>(P2);
+    PJ_CUDA(set_smem(hist_tuples_kernel<K>, hsmem));
+    hist_tuples_kernel<K><<<n_items * p->hist_split, HIST_THREADS, hsmem, st>>>(in, it, n_items, p->hist_split, f, P2,
+                                                                               L.P1, counts, tot);
+    PJ_CUDA(cudaGetLastError());
+    pj_status s;
+    const int W2 = pass2_wc(static_cast<int>(sizeof(K)), p);
+    if ((s = launch_scan<uint32_t>(counts, static_cast<int64_t>(P2) * n_items, static_cast<uint32_t>(W2), off, tiles,
+                                   ctr + (side == 0 ? CTR_BTILE2 : CTR_PTILE2), status, st)) != PJ_OK)
+        return s;
+    switch (W2) {
+    case 2: return launch_scatter_tuples<K, 2>(in, it, n_items, f, P2, off, out, cap, status, st);
+    case 4: return launch_scatter_tuples<K, 4>(in, it, n_items, f, P2, off, out, cap, status, st);
+    case 8: return launch_scatter_tuples<K, 8>(in, it, n_items, f, P2, off, out, cap, status, st);
+    case 16: return launch_scatter_tuples<K, 16>(in, it, n_items, f, P2, off, out, cap, status, st);
+    case 32: return launch_scatter_tuples<K, 32>(in, it, n_items, f, P2, off, out, cap, status, st);
+    default: return PJ_ERR_INVALID;
+    }
 }
 
 template <typename K>
@@ -687,10 +803,20 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
                                                                         const_cast<int32_t*>(hc.out.heavy_row));
         PJ_CUDA(cudaGetLastError());
     }
+    const bool two = p->passes == 2;
+    if (two && (s = partition_pass2<K>(p, L, 0, ws, reinterpret_cast<uint32_t*>(ws + L.b_tuples2), L.b_cap2, st)) !=
+                   PJ_OK)
+        return s;
     if ((s = partition_column<K>(static_cast<const K*>(d->probe_keys), d->n_probe, p, L, 1, ws,
                                  reinterpret_cast<uint32_t*>(ws + L.p_tuples), L.p_cap, E, PJ_STAGE_PROBE_HIST,
                                  st, hc)) != PJ_OK)
         return s;
+    if (two && (s = partition_pass2<K>(p, L, 1, ws, reinterpret_cast<uint32_t*>(ws + L.p_tuples2), L.p_cap2, st)) !=
+                   PJ_OK)
+        return s;
+    // the partitions the join reads: second-pass output for two-pass plans
+    const size_t jb_off = two ? L.b_off2 : L.b_off, jp_off = two ? L.p_off2 : L.p_off;
+    const int jb_items = two ? L.C : L.b_items, jp_items = two ? L.C : L.p_items;
     E.mark(PJ_STAGE_JOIN_PLAN, st);
     if (hc.hs) {  // the heavy pairs [0, H) precede every join chunk
         heavy_total_kernel<<<1, 32, 0, st>>>(hc.out.item_count, L.p_items, heavy_total,
@@ -702,7 +828,7 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     const bool hash_split = p->split_mode == PJ_SPLIT_HASH;
     const int position_chunk = std::max(16, cap_tuples / 16 * 16);
     join_items_kernel<<<(L.P + 255) / 256, 256, 0, st>>>(
-        reinterpret_cast<int64_t*>(ws + L.b_off), reinterpret_cast<int64_t*>(ws + L.p_off), L.b_items, L.p_items,
+        reinterpret_cast<int64_t*>(ws + jb_off), reinterpret_cast<int64_t*>(ws + jp_off), jb_items, jp_items,
         L.P, reinterpret_cast<int32_t*>(ws + L.b_tot), reinterpret_cast<int32_t*>(ws + L.p_tot),
         hash_split ? cap_tuples : position_chunk, p->probe_chunk, hash_split ? 1 : 0, MAX_SPLIT_LOG2,
         reinterpret_cast<int32_t*>(ws + L.split), reinterpret_cast<int64_t*>(ws + L.items), status);
@@ -716,14 +842,15 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     PJ_CUDA(cudaGetLastError());
 
     JoinArgs a{};
-    a.build_tuples = reinterpret_cast<const uint32_t*>(ws + L.b_tuples);
-    a.probe_tuples = reinterpret_cast<const uint32_t*>(ws + L.p_tuples);
-    a.build_off = reinterpret_cast<const int64_t*>(ws + L.b_off);
-    a.probe_off = reinterpret_cast<const int64_t*>(ws + L.p_off);
-    a.b_items = L.b_items;
-    a.p_items = L.p_items;
+    a.build_tuples = reinterpret_cast<const uint32_t*>(ws + (two ? L.b_tuples2 : L.b_tuples));
+    a.probe_tuples = reinterpret_cast<const uint32_t*>(ws + (two ? L.p_tuples2 : L.p_tuples));
+    a.build_off = reinterpret_cast<const int64_t*>(ws + jb_off);
+    a.probe_off = reinterpret_cast<const int64_t*>(ws + jp_off);
+    a.b_items = jb_items;
+    a.p_items = jp_items;
     a.P = L.P;
-    a.digit_bits = p->digit_mode == PJ_DIGIT_HASH ? p->bits1 + p->bits2 : 0;
+    // top hash bits the partition digits consumed
+    a.digit_bits = (p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0) + (two ? p->bits2 : 0);
     a.split = reinterpret_cast<const int32_t*>(ws + L.split);
     a.item_off = reinterpret_cast<const int64_t*>(ws + L.item_off);
     a.item_part = reinterpret_cast<const int32_t*>(ws + L.item_part);
@@ -883,6 +1010,19 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
             // partitions 7.2 ms, 4096 partitions 4.6 ms)
             bits = bits_for(ccap);
             while (bits < 16 && pick_w(bits + 1) != 0) ++bits;
+        }
+    }
+    if (pick_w(bits) == 0 && p->table_mode == PJ_TABLE_BUCKET) {
+        // beyond what one pass makes even for COMPACT tables: two passes
+        // (the reference's radix plan, main.cu:240-248), BUCKET tables
+        const int b1 = (bits + 1) / 2, b2 = bits - b1;
+        const int w = pick_w(b1);
+        if (b2 >= 1 && w != 0) {
+            p->passes = 2;
+            p->bits1 = b1;
+            p->bits2 = b2;
+            p->wc_tuples = w;
+            return PJ_OK;
         }
     }
     while (bits > 0 && pick_w(bits) == 0) --bits;  // still beyond: hash splits absorb the rest
@@ -1058,7 +1198,13 @@ pj_status pj_partitioned_capacity(int64_t n, int32_t key_bytes, const pj_plan* p
 {
     if (n < 0 || n > INT32_MAX || (key_bytes != 4 && key_bytes != 8) || !plan || !tuples) return PJ_ERR_INVALID;
     if (!valid_wc(key_bytes, plan->wc_tuples)) return PJ_ERR_INVALID;
-    *tuples = part_capacity(n, 1 << plan->bits1, scatter_items(plan), plan->wc_tuples);
+    pj_join_desc d{};
+    d.build_keys = reinterpret_cast<const void*>(16);
+    d.n_build = n;
+    d.key_bytes = key_bytes;
+    d.unique_build_keys = 1;
+    const Layout L = make_layout(&d, plan);
+    *tuples = plan->passes == 2 ? L.b_cap2 : L.b_cap;
     return PJ_OK;
 }
 
@@ -1082,15 +1228,22 @@ pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     uint8_t* w = static_cast<uint8_t*>(ws);
     PJ_CUDA(cudaMemsetAsync(w, 0, L.ctrl_end, st));
+    const bool two = plan->passes == 2;
+    uint32_t* first = two ? reinterpret_cast<uint32_t*>(w + L.b_tuples) : static_cast<uint32_t*>(tuples);
     if (key_bytes == 4)
-        s = partition_column<int32_t>(static_cast<const int32_t*>(keys), n, plan, L, 0, w, static_cast<uint32_t*>(tuples),
-                                      L.b_cap, StageEvents(), 0, st);
+        s = partition_column<int32_t>(static_cast<const int32_t*>(keys), n, plan, L, 0, w, first, L.b_cap,
+                                      StageEvents(), 0, st);
     else
-        s = partition_column<int64_t>(static_cast<const int64_t*>(keys), n, plan, L, 0, w, static_cast<uint32_t*>(tuples),
-                                      L.b_cap, StageEvents(), 0, st);
+        s = partition_column<int64_t>(static_cast<const int64_t*>(keys), n, plan, L, 0, w, first, L.b_cap,
+                                      StageEvents(), 0, st);
     if (s != PJ_OK) return s;
-    partition_bounds_kernel<<<(L.P + 1 + 255) / 256, 256, 0, st>>>(reinterpret_cast<int64_t*>(w + L.b_off), L.b_items,
-                                                                   L.P, offsets);
+    if (two) {
+        s = key_bytes == 4 ? partition_pass2<int32_t>(plan, L, 0, w, static_cast<uint32_t*>(tuples), L.b_cap2, st)
+                           : partition_pass2<int64_t>(plan, L, 0, w, static_cast<uint32_t*>(tuples), L.b_cap2, st);
+        if (s != PJ_OK) return s;
+    }
+    partition_bounds_kernel<<<(L.P + 1 + 255) / 256, 256, 0, st>>>(
+        reinterpret_cast<int64_t*>(w + (two ? L.b_off2 : L.b_off)), two ? L.C : L.b_items, L.P, offsets);
     PJ_CUDA(cudaGetLastError());
     return PJ_OK;
 }

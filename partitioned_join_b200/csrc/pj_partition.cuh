@@ -59,10 +59,10 @@ __device__ __forceinline__ void load_vec16(const K* p, K (&out)[Vec16<K>::N])
 }
 
 // Byte offset of the heavy table in the scatter's shared memory: after P
-// buffers of BW words and P {fill, cursor} pairs, rounded up to 16 bytes.
-__host__ __device__ constexpr size_t heavy_table_offset(int P, int BW)
+// buffers of capw words and P {fill, cursor} pairs, rounded up to 16 bytes.
+__host__ __device__ constexpr size_t heavy_table_offset(int P, int capw)
 {
-    return (static_cast<size_t>(P) * BW * 4 + static_cast<size_t>(P) * 8 + 15) & ~static_cast<size_t>(15);
+    return (static_cast<size_t>(P) * capw * 4 + static_cast<size_t>(P) * 8 + 15) & ~static_cast<size_t>(15);
 }
 
 // Output of heavy probe keys (heavy-key path).  The probe histogram counts,
@@ -365,31 +365,136 @@ __device__ __forceinline__ void wc_flush(const uint32_t* sbuf, uint32_t* gdst)
 
 
 
+// One round of the write-combining scatter: every thread places its V
+// tuples (words w, partition dv, ok = real) through the per-partition
+// buffers of cap tuples (a multiple of the group size W).  Phase A: a shared
+// atomic gives each tuple its slot in its partition's stream; slots below
+// cap go to the buffer.  Phase B: the tuple in the last slot of each
+// complete group inside the buffer flushes that group (one 32-byte store per
+// sector); tuples of complete groups past the buffer go straight out.
+// Phase C: the partial group after the last complete one moves to the
+// buffer's front and the holder of the last complete slot advances the
+// partition's cursor.  At every round's start a buffer holds fewer than W
+// tuples.  Every thread of the CTA calls it (three barriers).
+template <typename K, int W, int V>
+__device__ __forceinline__ void wc_place(const uint32_t (&w)[V][TupleTraits<K>::WORDS], const uint32_t (&dv)[V],
+                                         const bool (&ok)[V], uint32_t* buf, int cap, int2* fc,
+                                         uint32_t* __restrict__ out, uint32_t out_cap, uint32_t* __restrict__ status)
+{
+    constexpr int TW = WcTraits<K, W>::TW;
+    const int capw = cap * TW;
+    int s[V], F[V], Q[V];
+    // phase A
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        s[v] = ok[v] ? atomicAdd(&fc[dv[v]].x, 1) : -1;
+        if (ok[v] && s[v] < cap) store_words<TW>(buf + dv[v] * capw + s[v] * TW, w[v]);
+    }
+    __syncthreads();
+    // phase B: only the tuples at or past the first group's last slot act
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        if (s[v] >= W - 1) {
+            const int2 st = fc[dv[v]];
+            F[v] = st.x;
+            Q[v] = F[v] & ~(W - 1);
+            const uint32_t cur_p = static_cast<uint32_t>(st.y);
+            if (s[v] < cap) {
+                if ((s[v] & (W - 1)) == W - 1) {
+                    const int g0 = s[v] - (W - 1);  // first slot of the complete group
+                    const uint32_t pos = cur_p + static_cast<uint32_t>(g0);
+                    if (pos + static_cast<uint32_t>(W) <= out_cap)
+                        wc_flush<K, W>(buf + dv[v] * capw + g0 * TW, out + static_cast<size_t>(pos) * TW);
+                    else
+                        raise_status(status, ST_INTERNAL);
+                }
+            } else if (s[v] < Q[v]) {
+                const uint32_t pos = cur_p + static_cast<uint32_t>(s[v]);
+                if (pos < out_cap)
+                    store_words<TW>(out + static_cast<size_t>(pos) * TW, w[v]);
+                else
+                    raise_status(status, ST_INTERNAL);
+            }
+        }
+    }
+    __syncthreads();
+    // phase C: a slot past the first group exists only where a group
+    // completed (Q >= W), and then every slot from Q on was taken this round
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        if (s[v] >= W - 1 && Q[v] >= W) {
+            if (s[v] >= Q[v]) store_words<TW>(buf + dv[v] * capw + (s[v] - Q[v]) * TW, w[v]);
+            if (s[v] == Q[v] - 1) {
+                const int2 st = fc[dv[v]];
+                fc[dv[v]] = make_int2(F[v] - Q[v], st.y + Q[v]);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// End of an item: pad every partial buffer to W tuples, write it, and check
+// that each partition's cursor reached the end of its segment
+// [offsets[p * n_items + item], offsets[p * n_items + item + 1]).
+template <typename K, int W>
+__device__ __forceinline__ void wc_finish(int P, uint32_t* buf, int cap, int2* fc, uint32_t* __restrict__ out,
+                                          uint32_t out_cap,
+                                          const int64_t* __restrict__ offsets, int32_t n_items, int32_t item,
+                                          uint32_t* __restrict__ status)
+{
+    constexpr int TW = WcTraits<K, W>::TW;
+    // final flush: pad every partial group (fewer than W tuples, at the
+    // buffer's front) to W tuples and write it
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        const int fl = fc[p].x;
+        uint32_t cur_p = static_cast<uint32_t>(fc[p].y);
+        if (fl > 0) {
+            uint32_t* bq = buf + static_cast<size_t>(p) * cap * TW;
+            for (int q = fl; q < W; ++q) {
+                uint32_t pad[TW];
+#pragma unroll
+                for (int i = 0; i < TW; ++i) pad[i] = 0u;
+                pad[TW - 1] = static_cast<uint32_t>(PAD_ROW);
+                store_words<TW>(bq + q * TW, pad);
+            }
+            if (cur_p + static_cast<uint32_t>(W) <= out_cap)
+                wc_flush<K, W>(bq, out + static_cast<size_t>(cur_p) * TW);
+            else
+                raise_status(status, ST_INTERNAL);
+            cur_p += W;
+        }
+        if (cur_p != static_cast<uint32_t>(offsets[static_cast<int64_t>(p) * n_items + item + 1]))
+            raise_status(status, ST_INTERNAL);
+    }
+}
+
 // Scatter of a raw key column (row = key index).  V keys per thread per
 // round (whole 16-byte vectors), the next two rounds' vectors loaded while
-// the current round is processed.  Per partition the CTA keeps a W-tuple
-// buffer and a packed {fill, cursor} pair (one 64-bit shared access).
+// the current round is processed.  Per partition the CTA keeps a buffer of
+// cap tuples (whole groups of W) and a packed {fill, cursor} pair (one
+// 64-bit shared access).
 template <typename K, int THREADS, int V, int W, bool HASHD, bool HEAVY>
 __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __restrict__ keys, int64_t n,
                                                                   int64_t chunk, int32_t n_items, DigitFn f,
-                                                                  int32_t P, const int64_t* __restrict__ offsets,
+                                                                  int32_t P, int32_t cap,
+                                                                  const int64_t* __restrict__ offsets,
                                                                   uint32_t* __restrict__ out, uint32_t out_cap,
                                                                   uint32_t* __restrict__ status,
                                                                   typename HeavyArg<HEAVY>::type hs, HeavyOut ho)
 {
-    constexpr int TW = WcTraits<K, W>::TW, BW = WcTraits<K, W>::BW;
+    constexpr int TW = WcTraits<K, W>::TW;
     constexpr int VN = Vec16<K>::N;
     constexpr int NV = V / VN;  // vectors per thread per round
     static_assert(V % VN == 0, "V must be whole vectors");
     constexpr int ROUND = THREADS * V;
     extern __shared__ __align__(128) uint8_t smem[];
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
-    int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * BW);  // {fill, cursor}
+    int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * cap * TW);  // {fill, cursor}
     HeavyTable heavy;
     if constexpr (HEAVY) {
         // after the buffers and counters, on a 16-byte boundary (slots are
         // read as 16-byte words)
-        heavy.bind(smem + heavy_table_offset(P, BW));
+        heavy.bind(smem + heavy_table_offset(P, cap * TW));
         heavy.build<K>(hs, ho.heavy_row);  // ends with a barrier
     }
     const int lane = threadIdx.x & 31;
@@ -449,7 +554,6 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __res
 
             uint32_t w[V][TW];
             uint32_t dv[V];  // the tuple's partition
-            int s[V], F[V], Q[V];
             bool ok[V];
 #pragma unroll
             for (int j = 0; j < NV; ++j)
@@ -513,71 +617,147 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __res
                     }
                 }
             }
-            // phase A
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                s[v] = ok[v] ? atomicAdd(&fc[dv[v]].x, 1) : -1;
-                if (ok[v] && s[v] < W) store_words<TW>(buf + dv[v] * BW + s[v] * TW, w[v]);
-            }
-            __syncthreads();
-            // phase B: only the tuples at or past the buffer's last slot act
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                if (s[v] >= W - 1) {
-                    const int2 st = fc[dv[v]];
-                    F[v] = st.x;
-                    Q[v] = F[v] & ~(W - 1);
-                    const uint32_t cur_p = static_cast<uint32_t>(st.y);
-                    if (s[v] == W - 1) {
-                        if (cur_p + static_cast<uint32_t>(W) <= out_cap)
-                            wc_flush<K, W>(buf + dv[v] * BW, out + static_cast<size_t>(cur_p) * TW);
-                        else
-                            raise_status(status, ST_INTERNAL);
-                    } else if (s[v] < Q[v]) {
-                        const uint32_t pos = cur_p + static_cast<uint32_t>(s[v]);
-                        if (pos < out_cap)
-                            store_words<TW>(out + static_cast<size_t>(pos) * TW, w[v]);
-                        else
-                            raise_status(status, ST_INTERNAL);
-                    }
-                }
-            }
-            __syncthreads();
-            // phase C
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                if (s[v] >= W - 1) {
-                    if (s[v] >= Q[v] && s[v] >= W) store_words<TW>(buf + dv[v] * BW + (s[v] - Q[v]) * TW, w[v]);
-                    if (s[v] == W - 1) {
-                        const int2 st = fc[dv[v]];
-                        fc[dv[v]] = make_int2(F[v] - Q[v], st.y + Q[v]);
-                    }
-                }
-            }
-            __syncthreads();
+            wc_place<K, W, V>(w, dv, ok, buf, cap, fc, out, out_cap, status);
         }
-        // final flush: pad every partial buffer to W tuples and write it
-        for (int p = threadIdx.x; p < P; p += THREADS) {
-            const int fl = fc[p].x;
-            uint32_t cur_p = static_cast<uint32_t>(fc[p].y);
-            if (fl > 0) {
-                uint32_t* bq = buf + static_cast<size_t>(p) * BW;
-                for (int q = fl; q < W; ++q) {
-                    uint32_t pad[TW];
-#pragma unroll
-                    for (int i = 0; i < TW; ++i) pad[i] = 0u;
-                    pad[TW - 1] = static_cast<uint32_t>(PAD_ROW);
-                    store_words<TW>(bq + q * TW, pad);
-                }
-                if (cur_p + static_cast<uint32_t>(W) <= out_cap)
-                    wc_flush<K, W>(bq, out + static_cast<size_t>(cur_p) * TW);
-                else
-                    raise_status(status, ST_INTERNAL);
-                cur_p += W;
-            }
-            if (cur_p != static_cast<uint32_t>(offsets[static_cast<int64_t>(p) * n_items + item + 1]))
-                raise_status(status, ST_INTERNAL);
+        wc_finish<K, W>(P, buf, cap, fc, out, out_cap, offsets, n_items, item, status);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Second radix pass (two-pass plans): the tuples of each pass-one partition
+// are partitioned again by the next hash bits -- the reference's
+// histogram_pass_two / partition_pass_two (partition_kernels.cuh:329-563),
+// reading pass-one tuples instead of rewriting the input columns.
+// Item (p1, c) is the c-th of C slices of pass-one partition p1's tuples
+// [in_off[p1 * in_items], in_off[(p1 + 1) * in_items]); its tuples of sub-
+// partition p2 go to the segment [off[p2 * n_items + item], ...).  With
+// item = p1 * C + c that index is (p2 * P1 + p1) * C + c, so the join sees
+// partition q = p2 * P1 + p1 as one range over C segments.
+struct Pass2Items {
+    const int64_t* in_off;  // pass-one segment offsets
+    int32_t in_items;       // pass-one items
+    int32_t C;              // slices per pass-one partition
+};
+
+__device__ __forceinline__ void pass2_range(const Pass2Items& it, int item, int64_t& lo, int64_t& hi)
+{
+    const int p1 = item / it.C, c = item % it.C;
+    const int64_t start = it.in_off[static_cast<int64_t>(p1) * it.in_items];
+    const int64_t end = it.in_off[static_cast<int64_t>(p1 + 1) * it.in_items];
+    const int64_t per = (((end - start) + it.C - 1) / it.C + 15) & ~int64_t(15);
+    lo = start + c * per;
+    hi = lo + per < end ? lo + per : end;
+    if (lo > hi) lo = hi;
+}
+
+// tuple i's words and whether it is a real (not padding) tuple
+template <typename K>
+__device__ __forceinline__ bool load_tuple_words(const uint32_t* __restrict__ t, int64_t i,
+                                                 uint32_t (&w)[TupleTraits<K>::WORDS])
+{
+    if constexpr (TupleTraits<K>::WORDS == 2) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(t) + i);
+        w[0] = v.x;
+        w[1] = v.y;
+    } else {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(t) + i);
+        w[0] = v.x;
+        w[1] = v.y;
+        w[2] = v.z;
+        w[3] = v.w;
+    }
+    return static_cast<int32_t>(w[TupleTraits<K>::WORDS - 1]) != PAD_ROW;
+}
+
+// the stored hash of a tuple (word 0 for 4-byte keys, word 2 for 8-byte keys)
+template <typename K>
+__device__ __forceinline__ uint32_t tuple_hash(const uint32_t (&w)[TupleTraits<K>::WORDS])
+{
+    return TupleTraits<K>::WORDS == 2 ? w[0] : w[TupleTraits<K>::WORDS - 2];
+}
+
+// Pass-two histogram: counts_T[p2 * n_items + item] and totals[p2 * P1 + p1]
+// (zeroed by the caller).  Grid = n_items * hsplit CTAs.
+template <typename K>
+__global__ void __launch_bounds__(HIST_THREADS) hist_tuples_kernel(const uint32_t* __restrict__ tuples, Pass2Items it,
+                                                                   int32_t n_items, int32_t hsplit, DigitFn f,
+                                                                   int32_t P2, int32_t P1,
+                                                                   uint32_t* __restrict__ counts_T,
+                                                                   int32_t* __restrict__ totals)
+{
+    constexpr int TW = TupleTraits<K>::WORDS;
+    extern __shared__ __align__(16) uint32_t cnt[];
+    const int item = blockIdx.x / hsplit, part = blockIdx.x % hsplit;
+    for (int p = threadIdx.x; p < P2; p += HIST_THREADS) cnt[p] = 0;
+    __syncthreads();
+    int64_t lo, hi;
+    pass2_range(it, item, lo, hi);
+    const int64_t per = (((hi - lo) + hsplit - 1) / hsplit + 15) & ~int64_t(15);
+    int64_t s_lo = lo + part * per;
+    const int64_t s_hi = s_lo + per < hi ? s_lo + per : hi;
+    if (s_lo > s_hi) s_lo = s_hi;
+    for (int64_t i = s_lo + threadIdx.x; i < s_hi; i += HIST_THREADS) {
+        uint32_t w[TW];
+        if (load_tuple_words<K>(tuples, i, w)) atomicAdd(&cnt[(tuple_hash<K>(w) >> f.shift) & f.mask], 1u);
+    }
+    __syncthreads();
+    const int p1 = item / it.C;
+    for (int p = threadIdx.x; p < P2; p += HIST_THREADS) {
+        const uint32_t c = cnt[p];
+        if (c) {
+            atomicAdd(&counts_T[static_cast<int64_t>(p) * n_items + item], c);
+            atomicAdd(&totals[static_cast<int64_t>(p) * P1 + p1], static_cast<int32_t>(c));
         }
+    }
+}
+
+// Pass-two scatter: the pass-one tuples of each item, placed by the next
+// hash bits through the same write-combining buffers as the first pass.
+// VT tuples per thread per round, the next round's loaded ahead.
+template <typename K, int THREADS, int VT, int W>
+__global__ void __launch_bounds__(THREADS, 1) scatter_tuples_kernel(const uint32_t* __restrict__ in, Pass2Items it,
+                                                                    int32_t n_items, DigitFn f, int32_t P,
+                                                                    int32_t cap, const int64_t* __restrict__ offsets,
+                                                                    uint32_t* __restrict__ out, uint32_t out_cap,
+                                                                    uint32_t* __restrict__ status)
+{
+    constexpr int TW = WcTraits<K, W>::TW;
+    constexpr int ROUND = THREADS * VT;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
+    int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * cap * TW);
+    for (int32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+        for (int p = threadIdx.x; p < P; p += THREADS)
+            fc[p] = make_int2(0, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
+        __syncthreads();
+        int64_t lo, hi;
+        pass2_range(it, item, lo, hi);
+        uint32_t nw[VT][TW];
+        bool nok[VT];
+        auto load_round = [&](int64_t b) {
+#pragma unroll
+            for (int v = 0; v < VT; ++v) {
+                const int64_t i = b + static_cast<int64_t>(v) * THREADS + threadIdx.x;
+                nok[v] = i < hi && load_tuple_words<K>(in, i, nw[v]);
+            }
+        };
+        if (lo < hi) load_round(lo);
+        for (int64_t b = lo; b < hi; b += ROUND) {
+            uint32_t w[VT][TW];
+            uint32_t dv[VT];
+            bool ok[VT];
+#pragma unroll
+            for (int v = 0; v < VT; ++v) {
+                ok[v] = nok[v];
+#pragma unroll
+                for (int i = 0; i < TW; ++i) w[v][i] = nw[v][i];
+                dv[v] = (tuple_hash<K>(w[v]) >> f.shift) & f.mask;
+            }
+            if (b + ROUND < hi) load_round(b + ROUND);
+            wc_place<K, W, VT>(w, dv, ok, buf, cap, fc, out, out_cap, status);
+        }
+        wc_finish<K, W>(P, buf, cap, fc, out, out_cap, offsets, n_items, item, status);
         __syncthreads();
     }
 }

@@ -88,6 +88,7 @@ def test_partition_stage_exact(dtype, bits, mode):
     keys = rng.integers(info.min // 2, info.max // 2, size=n, dtype=dtype)
     plan = api.plan_default(n, n, np.dtype(dtype).itemsize)
     plan.bits1 = bits
+    plan.wc_tuples = 4 if dtype == np.int32 else 2   # the default's width may not fit 2^9 buffers
     plan.digit_mode = mode
     tuples, offsets = api.partition(dev(keys), plan)
     t = tuples.cpu().numpy()
@@ -113,6 +114,53 @@ def test_partition_stage_exact(dtype, bits, mode):
     part = np.repeat(np.arange(P), np.diff(off))
     d = oracle.digits(keys, mode, bits, 0, 0)
     assert np.array_equal(part[real], d[rows[real]])
+
+
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+@pytest.mark.parametrize("mode", [DIGIT_RAW, DIGIT_HASH])
+def test_two_pass_partition_stage_exact(dtype, mode):
+    rng = np.random.default_rng(31)
+    n = 300007
+    info = np.iinfo(dtype)
+    keys = rng.integers(info.min // 2, info.max // 2, size=n, dtype=dtype)
+    plan = api.plan_default(n, n, np.dtype(dtype).itemsize)
+    plan.passes, plan.bits1, plan.bits2, plan.digit_mode = 2, 3, 4, mode
+    tuples, offsets = api.partition(dev(keys), plan)
+    t, off = tuples.cpu().numpy(), offsets.cpu().numpy()
+    words = 2 if dtype == np.int32 else 4
+    P1, P2 = 8, 16
+    assert off.shape[0] == P1 * P2 + 1 and off[0] == 0 and np.all(np.diff(off) >= 0)
+    rec = t[: off[-1] * words].reshape(-1, words)
+    rows = rec[:, -1]
+    real = rows >= 0
+    assert np.array_equal(np.sort(rows[real]), np.arange(n))
+    # partition q = p2 * P1 + p1: p1 the first-pass digit, p2 the next hash bits
+    q = np.repeat(np.arange(P1 * P2), np.diff(off))
+    h = oracle.hash_keys(keys).astype(np.int64)
+    p1 = oracle.digits(keys, mode, 3, 0, 0).astype(np.int64)
+    hb = 3 if mode == DIGIT_HASH else 0
+    p2 = (h >> (32 - hb - 4)) & (P2 - 1)
+    assert np.array_equal(q[real], (p2 * P1 + p1)[rows[real]])
+
+
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
+@pytest.mark.parametrize("mode", [DIGIT_RAW, DIGIT_HASH])
+@pytest.mark.parametrize("unique", [True, False])
+def test_two_pass_join_matches_oracle(dtype, mode, unique):
+    b, p = datagen.config2(seed=32, n_build=400000, n_probe=700000)
+    b, p = b.astype(dtype), p.astype(dtype)
+    if not unique:
+        b = np.concatenate([b, b[:30000]])
+    plan = api.plan_default(b.shape[0], p.shape[0], np.dtype(dtype).itemsize, unique)
+    plan.passes, plan.bits1, plan.bits2, plan.digit_mode = 2, 3, 4, mode
+    plan.table_mode, plan.table_capacity = TABLE_BUCKET, 8192
+    br, pr = run(b, p, unique, plan)
+    assert pairs_equal(b, p, br, pr, unique)
+
+
+def test_two_pass_default_plan_for_large_builds():
+    plan = api.plan_default(1 << 29, 1 << 29, 4)
+    assert plan.passes == 2 and plan.bits1 + plan.bits2 >= 14 and plan.table_mode == TABLE_BUCKET
 
 
 # ---------------------------------------------------------------------------
@@ -226,7 +274,7 @@ def test_join_compact_default_plan_large_partitions():
     assert pairs_equal(b, p, br, pr)
 
 
-@pytest.mark.parametrize("w", [2, 4, 8])
+@pytest.mark.parametrize("w", [2, 4, 8, 16, 32])
 def test_join_wc_widths(w):
     b, p = datagen.config2(seed=18, n_build=200000, n_probe=300000)
     plan = api.plan_default(b.shape[0], p.shape[0], 4)
