@@ -59,7 +59,7 @@ __device__ __forceinline__ void load_vec16(const K* p, K (&out)[Vec16<K>::N])
 }
 
 // Byte offset of the heavy table in the scatter's shared memory: after P
-// buffers of capw words and P {fill, cursor} pairs, rounded up to 16 bytes.
+// buffers of capw words, P fill counts and P cursors, rounded up to 16 bytes.
 __host__ __device__ constexpr size_t heavy_table_offset(int P, int capw)
 {
     return (static_cast<size_t>(P) * capw * 4 + static_cast<size_t>(P) * 8 + 15) & ~static_cast<size_t>(15);
@@ -365,6 +365,23 @@ __device__ __forceinline__ void wc_flush(const uint32_t* sbuf, uint32_t* gdst)
 
 
 
+// Per-partition fill counts and output cursors of the write-combining
+// scatter: two 4-byte arrays after the buffers.
+struct WcState {
+    int* fill;
+    int* cur;
+    __device__ static WcState at(uint32_t* after_buffers, int P)
+    {
+        int* f = reinterpret_cast<int*>(after_buffers);
+        return WcState{f, f + P};
+    }
+    __device__ void init(int p, int cursor) const
+    {
+        fill[p] = 0;
+        cur[p] = cursor;
+    }
+};
+
 // One round of the write-combining scatter: every thread places its V
 // tuples (words w, partition dv, ok = real) through the per-partition
 // buffers of cap tuples (a multiple of the group size W).  Phase A: a shared
@@ -378,7 +395,7 @@ __device__ __forceinline__ void wc_flush(const uint32_t* sbuf, uint32_t* gdst)
 // tuples.  Every thread of the CTA calls it (three barriers).
 template <typename K, int W, int V>
 __device__ __forceinline__ void wc_place(const uint32_t (&w)[V][TupleTraits<K>::WORDS], const uint32_t (&dv)[V],
-                                         const bool (&ok)[V], uint32_t* buf, int cap, int2* fc,
+                                         const bool (&ok)[V], uint32_t* buf, int cap, WcState fc,
                                          uint32_t* __restrict__ out, uint32_t out_cap, uint32_t* __restrict__ status)
 {
     constexpr int TW = WcTraits<K, W>::TW;
@@ -387,7 +404,7 @@ __device__ __forceinline__ void wc_place(const uint32_t (&w)[V][TupleTraits<K>::
     // phase A
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-        s[v] = ok[v] ? atomicAdd(&fc[dv[v]].x, 1) : -1;
+        s[v] = ok[v] ? atomicAdd(&fc.fill[dv[v]], 1) : -1;
         if (ok[v] && s[v] < cap) store_words<TW>(buf + dv[v] * capw + s[v] * TW, w[v]);
     }
     __syncthreads();
@@ -395,10 +412,9 @@ __device__ __forceinline__ void wc_place(const uint32_t (&w)[V][TupleTraits<K>::
 #pragma unroll
     for (int v = 0; v < V; ++v) {
         if (s[v] >= W - 1) {
-            const int2 st = fc[dv[v]];
-            F[v] = st.x;
+            F[v] = fc.fill[dv[v]];
             Q[v] = F[v] & ~(W - 1);
-            const uint32_t cur_p = static_cast<uint32_t>(st.y);
+            const uint32_t cur_p = static_cast<uint32_t>(fc.cur[dv[v]]);
             if (s[v] < cap) {
                 if ((s[v] & (W - 1)) == W - 1) {
                     const int g0 = s[v] - (W - 1);  // first slot of the complete group
@@ -425,8 +441,8 @@ __device__ __forceinline__ void wc_place(const uint32_t (&w)[V][TupleTraits<K>::
         if (s[v] >= W - 1 && Q[v] >= W) {
             if (s[v] >= Q[v]) store_words<TW>(buf + dv[v] * capw + (s[v] - Q[v]) * TW, w[v]);
             if (s[v] == Q[v] - 1) {
-                const int2 st = fc[dv[v]];
-                fc[dv[v]] = make_int2(F[v] - Q[v], st.y + Q[v]);
+                fc.fill[dv[v]] = F[v] - Q[v];
+                fc.cur[dv[v]] += Q[v];
             }
         }
     }
@@ -437,7 +453,7 @@ __device__ __forceinline__ void wc_place(const uint32_t (&w)[V][TupleTraits<K>::
 // that each partition's cursor reached the end of its segment
 // [offsets[p * n_items + item], offsets[p * n_items + item + 1]).
 template <typename K, int W>
-__device__ __forceinline__ void wc_finish(int P, uint32_t* buf, int cap, int2* fc, uint32_t* __restrict__ out,
+__device__ __forceinline__ void wc_finish(int P, uint32_t* buf, int cap, WcState fc, uint32_t* __restrict__ out,
                                           uint32_t out_cap,
                                           const int64_t* __restrict__ offsets, int32_t n_items, int32_t item,
                                           uint32_t* __restrict__ status)
@@ -446,8 +462,8 @@ __device__ __forceinline__ void wc_finish(int P, uint32_t* buf, int cap, int2* f
     // final flush: pad every partial group (fewer than W tuples, at the
     // buffer's front) to W tuples and write it
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        const int fl = fc[p].x;
-        uint32_t cur_p = static_cast<uint32_t>(fc[p].y);
+        const int fl = fc.fill[p];
+        uint32_t cur_p = static_cast<uint32_t>(fc.cur[p]);
         if (fl > 0) {
             uint32_t* bq = buf + static_cast<size_t>(p) * cap * TW;
             for (int q = fl; q < W; ++q) {
@@ -471,8 +487,7 @@ __device__ __forceinline__ void wc_finish(int P, uint32_t* buf, int cap, int2* f
 // Scatter of a raw key column (row = key index).  V keys per thread per
 // round (whole 16-byte vectors), the next two rounds' vectors loaded while
 // the current round is processed.  Per partition the CTA keeps a buffer of
-// cap tuples (whole groups of W) and a packed {fill, cursor} pair (one
-// 64-bit shared access).
+// cap tuples (whole groups of W), a fill count and an output cursor.
 template <typename K, int THREADS, int V, int W, bool HASHD, bool HEAVY>
 __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __restrict__ keys, int64_t n,
                                                                   int64_t chunk, int32_t n_items, DigitFn f,
@@ -489,7 +504,7 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __res
     constexpr int ROUND = THREADS * V;
     extern __shared__ __align__(128) uint8_t smem[];
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
-    int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * cap * TW);  // {fill, cursor}
+    const WcState fc = WcState::at(buf + static_cast<size_t>(P) * cap * TW, P);
     HeavyTable heavy;
     if constexpr (HEAVY) {
         // after the buffers and counters, on a 16-byte boundary (slots are
@@ -503,7 +518,7 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_keys_kernel(const K* __res
     __shared__ uint32_t s_hcur;             // heavy pairs of this item so far
     for (int32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         for (int p = threadIdx.x; p < P; p += THREADS)
-            fc[p] = make_int2(0, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
+            fc.init(p, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
         if constexpr (HEAVY) {
             if (threadIdx.x < 32) {
                 unsigned long long sum = 0;
@@ -726,10 +741,10 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_tuples_kernel(const uint32
     constexpr int ROUND = THREADS * VT;
     extern __shared__ __align__(128) uint8_t smem[];
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
-    int2* fc = reinterpret_cast<int2*>(buf + static_cast<size_t>(P) * cap * TW);
+    const WcState fc = WcState::at(buf + static_cast<size_t>(P) * cap * TW, P);
     for (int32_t item = blockIdx.x; item < n_items; item += gridDim.x) {
         for (int p = threadIdx.x; p < P; p += THREADS)
-            fc[p] = make_int2(0, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
+            fc.init(p, static_cast<int>(offsets[static_cast<int64_t>(p) * n_items + item]));
         __syncthreads();
         int64_t lo, hi;
         pass2_range(it, item, lo, hi);
