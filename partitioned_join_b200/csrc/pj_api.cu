@@ -26,7 +26,10 @@ namespace {
 constexpr int SC_THREADS = 1024;
 constexpr int SC_V32 = 4, SC_V64 = 2;  // keys per thread per round (one 16-byte vector)
 #ifndef PJ_JOIN_THREADS
-constexpr int JN_THREADS = 1024;
+// 24 warps of up to 85 registers: the 1024-thread form (64 registers) spilled
+// in the probe loop; 2^27 x 2^27 int32 join 2.43 -> 2.37 ms, 2^26 x 2^28
+// int64 4.37 -> 3.73 ms (512, 640, 896 threads all measured slower)
+constexpr int JN_THREADS = 768;
 #else
 constexpr int JN_THREADS = PJ_JOIN_THREADS;
 #endif
