@@ -5,11 +5,11 @@ The native library (libpj.so) is built in-tree by
 `python -m partitioned_join_b200.build`; importing the package does not
 build it, and every operation raises if it is missing.
 """
-from ._lib import (DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, TABLE_BUCKET, TABLE_COMPACT,
+from ._lib import (DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, TABLE_BUCKET, TABLE_COMPACT, TABLE_EXACT,
                    TABLE_OPEN, JoinDesc, Output, PJError, Plan)
 
 __all__ = ["DIGIT_HASH", "DIGIT_RAW", "SLOT_FAST", "SLOT_REF", "SPLIT_HASH", "SPLIT_POSITION", "TABLE_BUCKET",
-           "TABLE_COMPACT", "TABLE_OPEN", "JoinDesc",
+           "TABLE_COMPACT", "TABLE_EXACT", "TABLE_OPEN", "JoinDesc",
            "Output", "PJError", "Plan", "api", "datagen"]
 
 

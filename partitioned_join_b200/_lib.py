@@ -13,7 +13,7 @@ OK, ERR_INVALID, ERR_CAPACITY, ERR_CUDA, ERR_TIMEOUT, ERR_WORKSPACE, ERR_OVERFLO
 DIGIT_RAW, DIGIT_HASH = 0, 1
 SLOT_FAST, SLOT_REF = 0, 1
 SPLIT_HASH, SPLIT_POSITION = 0, 1
-TABLE_BUCKET, TABLE_OPEN, TABLE_COMPACT = 0, 1, 2
+TABLE_BUCKET, TABLE_OPEN, TABLE_COMPACT, TABLE_EXACT = 0, 1, 2, 3
 NOALLOC_SCRATCH_BYTES = 64 << 20  # PJ_NOALLOC_SCRATCH_BYTES
 MAX_HEAVY = 256                   # PJ_MAX_HEAVY
 STAGES = ["build_hist", "build_scan", "build_scatter", "probe_hist", "probe_scan", "probe_scatter", "join_plan",

@@ -347,8 +347,10 @@ int run(Options& o)
         }
         std::cout << "    B200 plan            = " << (1 << plan.bits1) << " partitions ("
                   << (plan.digit_mode == PJ_DIGIT_RAW ? "raw key bits" : "hash bits") << "), "
-                  << (plan.table_mode == PJ_TABLE_BUCKET ? "bucket" : plan.table_mode == PJ_TABLE_COMPACT ? "compact"
-                                                                                                       : "open")
+                  << (plan.table_mode == PJ_TABLE_BUCKET    ? "bucket"
+                      : plan.table_mode == PJ_TABLE_COMPACT ? "compact"
+                      : plan.table_mode == PJ_TABLE_EXACT   ? "exact"
+                                                            : "open")
                   << " tables of " << plan.table_capacity << std::endl;
         std::cout << "[*] Performing join" << std::endl;
     }

@@ -141,19 +141,59 @@ bool sector_wc(int key_bytes, int W) { return valid_wc(key_bytes, W) && (W * tup
 int bucket_nb_log2(int cap) { return std::max(1, ilog2_floor(std::max(2, cap / 2))); }
 
 template <typename K>
-size_t join_smem_k(int table_mode, int cap)
+size_t join_smem_k(int table_mode, int cap, int nb)
 {
-    const int nb = bucket_nb_log2(cap);
     switch (table_mode) {
     case PJ_TABLE_BUCKET: return JoinSmem<K, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS);
     case PJ_TABLE_COMPACT: return JoinSmem<K, TABLE_COMPACT>::bytes(cap, nb, JN_THREADS);
+    case PJ_TABLE_EXACT: return JoinSmem<K, TABLE_EXACT>::bytes(cap, nb, JN_THREADS);
     default: return JoinSmem<K, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
     }
 }
 
-size_t join_smem(int key_bytes, int table_mode, int cap)
+// Shared memory of a join CTA for a table of cap tuples and 2^nb buckets
+// (nb < 0: the default bucket count for cap).
+size_t join_smem(int key_bytes, int table_mode, int cap, int nb = -1)
 {
-    return key_bytes == 4 ? join_smem_k<int32_t>(table_mode, cap) : join_smem_k<int64_t>(table_mode, cap);
+    if (nb < 0) nb = bucket_nb_log2(cap);
+    return key_bytes == 4 ? join_smem_k<int32_t>(table_mode, cap, nb) : join_smem_k<int64_t>(table_mode, cap, nb);
+}
+
+// EXACT tables (4-byte keys): an entry holds the build row in its low
+// exact_row_bits bits and the hash bits above the bucket bits in the rest.
+// With the partition's hash digits and the bucket they fix the whole
+// MurmurHash3 value, which for a 4-byte key is a bijection of the key, so a
+// lookup needs no build-tuple load.  That takes 2^nb buckets with
+// digit bits + nb + (32 - row bits) >= 32.
+int exact_row_bits(int64_t n_build)
+{
+    int r = 1;
+    while (r < 31 && (int64_t(1) << r) < n_build) ++r;
+    return r;
+}
+
+int plan_digit_bits(const pj_plan* p)
+{
+    return (p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0) + (p->passes == 2 ? p->bits2 : 0);
+}
+
+// log2 of the bucket count of the plan's tables
+int table_nb_log2(int64_t n_build, const pj_plan* p)
+{
+    const int nb = bucket_nb_log2(p->table_capacity);
+    if (p->table_mode != PJ_TABLE_EXACT) return nb;
+    return std::max(nb, exact_row_bits(n_build) - plan_digit_bits(p));
+}
+
+// Largest EXACT capacity (a multiple of 128 tuples) with at least 2^nb_min
+// buckets; 0 if none fits shared memory.
+int exact_table_capacity(int nb_min)
+{
+    if (nb_min > 20) return 0;
+    int best = 0;
+    for (int cap = 128; cap <= MAX_BUCKET_CAP; cap += 128)
+        if (join_smem(4, PJ_TABLE_EXACT, cap, std::max(bucket_nb_log2(cap), nb_min)) <= smem_limit()) best = cap;
+    return best;
 }
 
 int max_table_capacity(int key_bytes, int table_mode)
@@ -193,12 +233,19 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (!valid_wc(d->key_bytes, p->wc_tuples)) return PJ_ERR_INVALID;
     if (scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) > smem_limit()) return PJ_ERR_INVALID;
     if (p->digit_mode != PJ_DIGIT_RAW && p->digit_mode != PJ_DIGIT_HASH) return PJ_ERR_INVALID;
-    if (p->table_mode != PJ_TABLE_BUCKET && p->table_mode != PJ_TABLE_OPEN && p->table_mode != PJ_TABLE_COMPACT)
+    if (p->table_mode != PJ_TABLE_BUCKET && p->table_mode != PJ_TABLE_OPEN && p->table_mode != PJ_TABLE_COMPACT &&
+        p->table_mode != PJ_TABLE_EXACT)
         return PJ_ERR_INVALID;
     if (p->slot_mode != PJ_SLOT_FAST && p->slot_mode != PJ_SLOT_REF) return PJ_ERR_INVALID;
     if (p->split_mode != PJ_SPLIT_HASH && p->split_mode != PJ_SPLIT_POSITION) return PJ_ERR_INVALID;
-    if (p->table_capacity < 64 || p->table_capacity > max_table_capacity(d->key_bytes, p->table_mode))
+    if (p->table_mode == PJ_TABLE_EXACT) {
+        // the hash is a bijection of the key for 4-byte keys only
+        if (d->key_bytes != 4 || p->table_capacity < 64 || p->table_capacity > MAX_BUCKET_CAP) return PJ_ERR_INVALID;
+        const int nb = table_nb_log2(d->n_build, p);
+        if (nb > 20 || join_smem(4, PJ_TABLE_EXACT, p->table_capacity, nb) > smem_limit()) return PJ_ERR_INVALID;
+    } else if (p->table_capacity < 64 || p->table_capacity > max_table_capacity(d->key_bytes, p->table_mode)) {
         return PJ_ERR_INVALID;
+    }
     if (p->probe_chunk < 16 || (p->probe_chunk & 15)) return PJ_ERR_INVALID;
     if (p->scatter_ctas_per_sm < 1 || p->scatter_ctas_per_sm > 8) return PJ_ERR_INVALID;
     if (p->hist_split < 1 || p->hist_split > 16) return PJ_ERR_INVALID;
@@ -207,8 +254,8 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (p->n_heavy > 0 && scatter_smem(d->key_bytes, p->wc_tuples, 1 << p->bits1) + HeavyTable::BYTES + 16 > smem_limit())
         return PJ_ERR_INVALID;  // the probe scatter also holds the heavy table
     // hash bits: digits + hash split + bucket/slot bits must fit 32
-    const int digit_bits = (p->digit_mode == PJ_DIGIT_HASH ? p->bits1 : 0) + (p->passes == 2 ? p->bits2 : 0);
-    const int slot_bits = p->table_mode != PJ_TABLE_OPEN ? bucket_nb_log2(p->table_capacity) : 12;
+    const int digit_bits = plan_digit_bits(p);
+    const int slot_bits = p->table_mode != PJ_TABLE_OPEN ? table_nb_log2(d->n_build, p) : 12;
     // digits and bucket bits disjoint; the bits of a hash split (below the
     // digits) may overlap the bucket bits: pieces stay exact, buckets coarser
     if (digit_bits + slot_bits > 32 || digit_bits + MAX_SPLIT_LOG2 > 31) return PJ_ERR_INVALID;
@@ -673,6 +720,10 @@ pj_status launch_join(const JoinArgs& a, int table_mode, bool unique, bool hash_
 {
     if (table_mode == PJ_TABLE_BUCKET) return launch_join_tab<K, TABLE_BUCKET>(a, unique, hash_split, false, st);
     if (table_mode == PJ_TABLE_COMPACT) return launch_join_tab<K, TABLE_COMPACT>(a, unique, hash_split, false, st);
+    if (table_mode == PJ_TABLE_EXACT) {
+        if constexpr (sizeof(K) == 4) return launch_join_tab<K, TABLE_EXACT>(a, unique, hash_split, false, st);
+        return PJ_ERR_INVALID;  // check_plan admits EXACT tables for 4-byte keys only
+    }
     return launch_join_tab<K, TABLE_OPEN>(a, unique, hash_split, slot_ref, st);
 }
 
@@ -860,7 +911,8 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
     a.max_items = L.max_items;
     a.queue = ctr + CTR_QUEUE;
     a.cap = p->table_capacity;
-    a.nb_log2 = bucket_nb_log2(p->table_capacity);
+    a.nb_log2 = table_nb_log2(d->n_build, p);
+    a.row_bits = exact_row_bits(d->n_build);
     a.probe_chunk = p->probe_chunk;
     a.position_chunk = position_chunk;
     a.out_build = out_b;
@@ -1032,6 +1084,16 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     p->bits1 = bits;
     p->wc_tuples = pick_w(bits);
     if (p->wc_tuples == 0) p->wc_tuples = d->key_bytes == 4 ? 4 : 8;
+    if (d->key_bytes == 4 && p->table_mode == PJ_TABLE_COMPACT) {
+        // EXACT tables (no build-tuple loads) where the expected largest
+        // hashed partition (mean + 4 standard deviations) fits one
+        const double m = static_cast<double>(d->n_build) / static_cast<double>(int64_t(1) << bits);
+        const int cap_e = exact_table_capacity(exact_row_bits(d->n_build) - bits);
+        if (cap_e > 0 && m + 4.0 * std::sqrt(m) + 1.0 <= cap_e) {
+            p->table_mode = PJ_TABLE_EXACT;
+            p->table_capacity = cap_e;
+        }
+    }
     return PJ_OK;
 }
 
@@ -1309,6 +1371,11 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
         raw_max = std::max<int64_t>(raw_max, host[i]);
         hash_max = std::max<int64_t>(hash_max, host[P + i]);
     }
+    // (an EXACT default is decided again below from the hashed partitions)
+    if (p.table_mode == PJ_TABLE_EXACT) {
+        p.table_mode = PJ_TABLE_COMPACT;
+        p.table_capacity = max_table_capacity(d->key_bytes, PJ_TABLE_COMPACT);
+    }
     // Raw key bits are free to compute: keep them (the reference's digits)
     // when their largest partition is no worse than the hashed one's.
     p.digit_mode = raw_max <= hash_max ? PJ_DIGIT_RAW : PJ_DIGIT_HASH;
@@ -1319,10 +1386,22 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
         p.table_mode = PJ_TABLE_BUCKET;
         p.table_capacity = max_table_capacity(d->key_bytes, PJ_TABLE_BUCKET);
     }
+    // 4-byte keys: EXACT tables instead of COMPACT ones (no build-tuple
+    // loads) where hash digits keep the largest partition within one
+    int64_t mx_plan = mx;
+    if (d->key_bytes == 4 && p.passes == 1 && p.table_mode == PJ_TABLE_COMPACT) {
+        const int cap_e = exact_table_capacity(exact_row_bits(d->n_build) - p.bits1);
+        if (cap_e > 0 && hash_max <= cap_e) {
+            p.table_mode = PJ_TABLE_EXACT;
+            p.digit_mode = PJ_DIGIT_HASH;
+            p.table_capacity = cap_e;
+            mx_plan = hash_max;
+        }
+    }
     const int64_t cap = table_tuples(&p);
     // Hash splits cannot separate repeated keys: a partition beyond what
     // 2^MAX_SPLIT_LOG2 tables hold (duplicates) takes the position split.
-    if (mx > cap * (int64_t(1) << MAX_SPLIT_LOG2) / 2) p.split_mode = PJ_SPLIT_POSITION;
+    if (mx_plan > cap * (int64_t(1) << MAX_SPLIT_LOG2) / 2) p.split_mode = PJ_SPLIT_POSITION;
     *plan = p;
     return PJ_OK;
 }

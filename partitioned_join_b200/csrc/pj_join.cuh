@@ -50,7 +50,7 @@
 namespace pj {
 
 constexpr uint32_t EMPTY_ROW = 0xffffffffu;
-enum : int { TABLE_BUCKET = 0, TABLE_OPEN = 1, TABLE_COMPACT = 2 };
+enum : int { TABLE_BUCKET = 0, TABLE_OPEN = 1, TABLE_COMPACT = 2, TABLE_EXACT = 3 };
 constexpr int64_t COMPACT_RANGE = 65536;  // build range a COMPACT entry's index can address
 
 struct JoinArgs {
@@ -68,7 +68,8 @@ struct JoinArgs {
     int64_t max_items;
     uint32_t* queue;            // item counter (zeroed)
     int32_t cap;                // build tuples one table holds (BUCKET) / slots (OPEN)
-    int32_t nb_log2;            // BUCKET: log2 of the bucket count
+    int32_t nb_log2;            // BUCKET, COMPACT, EXACT: log2 of the bucket count
+    int32_t row_bits;           // EXACT: low bits of an entry holding the build row
     int32_t probe_chunk;        // tuples
     int32_t position_chunk;     // build tuples per position split piece
     int32_t* out_build;         // nullptr: count only
@@ -302,7 +303,9 @@ struct JoinSmem {
     // table bytes for capacity cap (BUCKET: tuples; OPEN: slots) and 2^nb_log2 buckets
     __host__ __device__ static size_t entries_bytes(int cap)
     {
-        const size_t e = TABLE == TABLE_OPEN ? (sizeof(K) == 4 ? 8 : 12) : TABLE == TABLE_COMPACT ? 4 : Entry<K>::BYTES;
+        const size_t e = TABLE == TABLE_OPEN                                    ? (sizeof(K) == 4 ? 8 : 12)
+                         : (TABLE == TABLE_COMPACT || TABLE == TABLE_EXACT) ? 4
+                                                                            : Entry<K>::BYTES;
         return (static_cast<size_t>(cap) * e + 127) & ~size_t(127);
     }
     __host__ __device__ static size_t table_bytes(int cap, int nb_log2)
@@ -493,6 +496,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         };
         auto bucket_of = [&](uint32_t h) -> uint32_t { return h & nb_mask; };
         auto finger_of = [&](uint32_t h) -> uint32_t { return (h >> a.nb_log2) & 0xffffu; };
+        // EXACT entries: (hash bits above the bucket bits) << row_bits | build row;
+        // with the digits' and the bucket's bits they fix the whole hash
+        const uint32_t x_rmask = (1u << a.row_bits) - 1u;
+        auto xfinger_of = [&](uint32_t h) -> uint32_t { return (h >> a.nb_log2) & (0xffffffffu >> a.row_bits); };
         auto slot_of = [&](uint32_t h) -> uint32_t {
             return SLOT_REF ? slot_ref(h, a.cap) : slot_fast(h, skip, static_cast<uint32_t>(a.cap));
         };
@@ -573,6 +580,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             const int pos = static_cast<int>((b & 1u) ? (old >> 16) : (old & 0xffffu));
                             if constexpr (TABLE == TABLE_COMPACT)
                                 ctab[pos] = (finger_of(h[u]) << 16) | static_cast<uint32_t>(i0 + u * THREADS - b_lo);
+                            else if constexpr (TABLE == TABLE_EXACT)
+                                ctab[pos] = (xfinger_of(h[u]) << a.row_bits) | static_cast<uint32_t>(r[u]);
                             else
                                 E::put(table, pos, k[u], r[u]);
                         }
@@ -612,10 +621,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         }
 
         // the next item's build side streams into L2 while this item probes
-        // (not for COMPACT tables: their 32 K-tuple build ranges were evicted
+        // (not for COMPACT or EXACT tables: their 32 K-tuple build ranges were evicted
         // again before use -- 2^27 x 2^27 int32: 0.83 GB more DRAM reads and
         // no time gained, while 16 K-tuple BUCKET ranges gain 8% at 2^25)
-        if (TABLE != TABLE_COMPACT && threadIdx.x == 0 && next_p >= 0 && next_p != p) {
+        if (TABLE != TABLE_COMPACT && TABLE != TABLE_EXACT && threadIdx.x == 0 && next_p >= 0 && next_p != p) {
             const int64_t nb_lo = a.build_off[static_cast<int64_t>(next_p) * a.b_items];
             const int64_t nb_hi = a.build_off[static_cast<int64_t>(next_p + 1) * a.b_items];
             const int64_t nbytes = (nb_hi - nb_lo) * TV::WORDS * 4;
@@ -677,6 +686,18 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                                     brow_u = static_cast<uint32_t>(br);
                                     break;
                                 }
+                            }
+                        }
+                        if (!found || UNIQUE) live_u = false;
+                    } else if constexpr (TABLE == TABLE_EXACT) {
+                        const uint32_t fq = xfinger_of(h[u]);
+                        while (at_u < end_u) {
+                            const uint32_t e = ctab[at_u];
+                            ++at_u;
+                            if ((e >> a.row_bits) == fq) {  // the whole hash, so the key, is equal
+                                found = true;
+                                brow_u = e & x_rmask;
+                                break;
                             }
                         }
                         if (!found || UNIQUE) live_u = false;
@@ -788,6 +809,59 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             }
                         }
                         if (!__any_sync(0xffffffffu, again)) break;
+                    }
+                    int c = 0;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) c += emit[u] ? 1 : 0;
+                    append(c, [&](int at_stage) {
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+                            if (emit[u]) {
+                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
+                                stage_p[at_stage] = r[u];
+                                ++at_stage;
+                            }
+                    });
+                } else if constexpr (UNIQUE && TABLE == TABLE_EXACT) {
+                    // every tuple matches at most once, and an entry's bits decide
+                    // it: the U tuples walk their buckets in lockstep, no loads
+                    bool emit[U], live[U];
+                    uint32_t brow[U], fq[U];
+                    int at[U], end[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        emit[u] = false;
+                        brow[u] = 0;
+                        fq[u] = xfinger_of(h[u]);
+                        live[u] = r[u] >= 0 && in_piece(h[u]);
+                        at[u] = end[u] = 0;
+                        if (live[u]) {
+                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t wb = ends[b >> 1];
+                            const uint32_t wa = b == 0 ? 0u : ends[(b - 1) >> 1];
+                            end[u] = static_cast<int>((wb >> ((b & 1u) * 16)) & 0xffffu);
+                            at[u] = b == 0 ? 0 : static_cast<int>((wa >> (((b - 1) & 1u) * 16)) & 0xffffu);
+                            live[u] = at[u] < end[u];
+                        }
+                    }
+                    for (;;) {
+                        bool any = false;
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            if (live[u]) {
+                                const uint32_t e = ctab[at[u]];
+                                ++at[u];
+                                if ((e >> a.row_bits) == fq[u]) {
+                                    emit[u] = true;
+                                    brow[u] = e & x_rmask;
+                                    live[u] = false;
+                                } else {
+                                    live[u] = at[u] < end[u];
+                                }
+                            }
+                            any |= live[u];
+                        }
+                        if (!any) break;
                     }
                     int c = 0;
 #pragma unroll

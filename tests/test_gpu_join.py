@@ -6,7 +6,7 @@ import torch
 
 from oracle import oracle
 from partitioned_join_b200 import (DIGIT_HASH, DIGIT_RAW, SLOT_FAST, SLOT_REF, SPLIT_HASH, SPLIT_POSITION, TABLE_BUCKET,
-                                   TABLE_COMPACT, TABLE_OPEN, PJError)
+                                   TABLE_COMPACT, TABLE_EXACT, TABLE_OPEN, PJError)
 from partitioned_join_b200 import api, datagen
 
 pytestmark = pytest.mark.gpu
@@ -261,6 +261,70 @@ def test_join_compact_fingerprint_collisions(dtype, unique):
     plan.table_capacity = 256                      # 2^7 buckets
     br, pr = run(build, probe, unique, plan)
     assert pairs_equal(build, probe, br, pr, unique)
+
+
+@pytest.mark.parametrize("unique", [True, False])
+@pytest.mark.parametrize("split", [SPLIT_HASH, SPLIT_POSITION])
+@pytest.mark.parametrize("n_build", [4096, 4097, 300007])
+def test_join_exact_tables_match_oracle(unique, split, n_build):
+    # EXACT entries hold the build row in the low bits (12, 13 and 19 row
+    # bits here) and the hash bits above the bucket bits; small tables force
+    # several pieces per partition
+    rng = np.random.default_rng(n_build)
+    b = rng.permutation(np.arange(1, 3 * n_build, 3, dtype=np.int64))[:n_build].astype(np.int32)
+    if not unique:
+        b[: n_build // 10] = b[n_build // 10: 2 * (n_build // 10)]
+    p = np.concatenate([rng.choice(b, 2 * n_build), rng.integers(-(1 << 31), (1 << 31) - 1, n_build)]).astype(np.int32)
+    plan = api.plan_default(n_build, p.shape[0], 4, unique)
+    plan.table_mode, plan.digit_mode, plan.split_mode = TABLE_EXACT, DIGIT_HASH, split
+    plan.bits1 = 4
+    plan.wc_tuples = 4
+    plan.table_capacity = 2048
+    plan.probe_chunk = 4096
+    br, pr = run(b, p, unique, plan)
+    assert pairs_equal(b, p, br, pr, unique)
+
+
+def test_join_exact_tables_hash_twins():
+    # keys whose hashes agree on all bits below the partition digits: the
+    # digits alone tell them apart, and EXACT entries must not confuse them
+    keys = (np.arange(1, 1 << 22, dtype=np.int64) * 2654435761 + 12345).astype(np.int32)
+    h = oracle.hash_keys(keys).astype(np.int64)
+    low = h & ((1 << 26) - 1)
+    order = np.argsort(low, kind="stable")
+    ls = low[order]
+    same = np.nonzero(ls[1:] == ls[:-1])[0]
+    a, c = keys[order[same]], keys[order[same + 1]]
+    keep = np.unique(np.concatenate([a, c]), return_index=True)[1]
+    twins = np.concatenate([a, c])[np.sort(keep)]
+    assert len(twins) > 100
+    build = twins[::2]
+    probe = np.concatenate([twins, keys[:5000]])
+    build = np.unique(build)
+    plan = api.plan_default(build.shape[0], probe.shape[0], 4)
+    plan.table_mode, plan.digit_mode, plan.bits1, plan.wc_tuples = TABLE_EXACT, DIGIT_HASH, 6, 4
+    plan.table_capacity = 1024
+    br, pr = run(build, probe, True, plan)
+    assert pairs_equal(build, probe, br, pr)
+
+
+def test_join_exact_tables_planned_for_large_int32_builds():
+    assert api.plan_default(1 << 27, 1 << 27, 4).table_mode == TABLE_EXACT
+    assert api.plan_default(1 << 27, 1 << 27, 8).table_mode == TABLE_COMPACT
+
+
+def test_join_exact_tables_rejected_where_inexact():
+    b = np.arange(1, 1000, dtype=np.int64)
+    plan = api.plan_default(b.shape[0], b.shape[0], 8)
+    plan.table_mode, plan.digit_mode, plan.table_capacity = TABLE_EXACT, DIGIT_HASH, 1024
+    with pytest.raises(PJError):             # 8-byte keys: the hash is not a bijection
+        run(b, b, True, plan)
+    b32 = np.arange(1, 1 << 20, dtype=np.int32)
+    plan = api.plan_default(b32.shape[0], b32.shape[0], 4)
+    plan.table_mode, plan.digit_mode, plan.bits1, plan.wc_tuples = TABLE_EXACT, DIGIT_RAW, 0, 4
+    plan.table_capacity = 1024
+    with pytest.raises(PJError):             # 2^20 buckets needed: no room
+        run(b32, b32, True, plan)
 
 
 def test_join_compact_default_plan_large_partitions():
