@@ -285,6 +285,31 @@ def test_join_exact_tables_match_oracle(unique, split, n_build):
     assert pairs_equal(b, p, br, pr, unique)
 
 
+@pytest.mark.parametrize("mode", [DIGIT_RAW, DIGIT_HASH])
+def test_join_exact_tables_two_pass(mode):
+    # the join partition of a two-pass plan fixes bits2 hash bits (and the
+    # bits1 above them with hash digits): EXACT entries count on them
+    b, p = datagen.config2(seed=36, n_build=400000, n_probe=700000)
+    plan = api.plan_default(b.shape[0], p.shape[0], 4)
+    plan.passes, plan.bits1, plan.bits2, plan.digit_mode = 2, 4, 6, mode
+    plan.table_mode, plan.table_capacity = TABLE_EXACT, 4096
+    br, pr = run(b, p, True, plan)
+    assert pairs_equal(b, p, br, pr)
+
+
+def test_join_exact_tables_with_heavy_keys():
+    rng = np.random.default_rng(37)
+    b = rng.permutation(400000).astype(np.int32)
+    p = np.concatenate([rng.integers(0, 500000, size=600000), np.full(200000, 17), np.full(50000, 450001)]).astype(np.int32)
+    rng.shuffle(p)
+    plan = api.plan_default(b.shape[0], p.shape[0], 4)
+    plan.table_mode, plan.digit_mode, plan.bits1, plan.wc_tuples = TABLE_EXACT, DIGIT_HASH, 5, 4
+    plan.table_capacity = 16384
+    plan.set_heavy([17, 450001])
+    br, pr = run(b, p, True, plan)
+    assert pairs_equal(b, p, br, pr)
+
+
 def test_join_exact_tables_hash_twins():
     # keys whose hashes agree on all bits below the partition digits: the
     # digits alone tell them apart, and EXACT entries must not confuse them
