@@ -106,12 +106,13 @@ enum {
     PJ_TABLE_COMPACT = 2, /* bucket order with 4-byte entries (hash fingerprint and
                              index of the build tuple): ~2x the tuples per table;
                              a build range must stay within 65536 tuples */
-    PJ_TABLE_EXACT = 3    /* 4-byte keys only: bucket order with 4-byte entries that
-                             hold the build row and the hash bits neither the hash
-                             digits nor the bucket fix (MurmurHash3 of a 4-byte key
-                             is a bijection), so a lookup loads no build tuple;
-                             needs 2^nb buckets with hash digit bits + nb >= the
-                             bits of n_build - 1, so hash digits in practice */
+    PJ_TABLE_EXACT = 3    /* bucket order with entries that hold the build row and
+                             the hash bits neither the hash digits nor the bucket
+                             fix (4 bytes; 8 with an 8-byte key's low word): with
+                             them the entry fixes the key, so a lookup loads no
+                             build tuple; needs 2^nb buckets with hash digit
+                             bits + nb >= the bits of n_build - 1, so hash digits
+                             in practice */
 };
 
 /* Most heavy probe keys a plan can name. */

@@ -159,11 +159,12 @@ size_t join_smem(int key_bytes, int table_mode, int cap, int nb = -1)
     return key_bytes == 4 ? join_smem_k<int32_t>(table_mode, cap, nb) : join_smem_k<int64_t>(table_mode, cap, nb);
 }
 
-// EXACT tables (4-byte keys): an entry holds the build row in its low
-// exact_row_bits bits and the hash bits above the bucket bits in the rest.
-// With the partition's hash digits and the bucket they fix the whole
-// MurmurHash3 value, which for a 4-byte key is a bijection of the key, so a
-// lookup needs no build-tuple load.  That takes 2^nb buckets with
+// EXACT tables: an entry holds the build row in its low exact_row_bits
+// bits and the hash bits above the bucket bits in the rest (8-byte keys:
+// beside the key's low word).  With the partition's hash digits and the
+// bucket they fix the whole MurmurHash3 value, which fixes a 4-byte key
+// (a bijection) and, with the low word, an 8-byte key, so a lookup needs no
+// build-tuple load.  That takes 2^nb buckets with
 // digit bits + nb + (32 - row bits) >= 32.
 int exact_row_bits(int64_t n_build)
 {
@@ -187,12 +188,12 @@ int table_nb_log2(int64_t n_build, const pj_plan* p)
 
 // Largest EXACT capacity (a multiple of 128 tuples) with at least 2^nb_min
 // buckets; 0 if none fits shared memory.
-int exact_table_capacity(int nb_min)
+int exact_table_capacity(int key_bytes, int nb_min)
 {
     if (nb_min > 20) return 0;
     int best = 0;
     for (int cap = 128; cap <= MAX_BUCKET_CAP; cap += 128)
-        if (join_smem(4, PJ_TABLE_EXACT, cap, std::max(bucket_nb_log2(cap), nb_min)) <= smem_limit()) best = cap;
+        if (join_smem(key_bytes, PJ_TABLE_EXACT, cap, std::max(bucket_nb_log2(cap), nb_min)) <= smem_limit()) best = cap;
     return best;
 }
 
@@ -239,10 +240,10 @@ pj_status check_plan(const pj_join_desc* d, const pj_plan* p)
     if (p->slot_mode != PJ_SLOT_FAST && p->slot_mode != PJ_SLOT_REF) return PJ_ERR_INVALID;
     if (p->split_mode != PJ_SPLIT_HASH && p->split_mode != PJ_SPLIT_POSITION) return PJ_ERR_INVALID;
     if (p->table_mode == PJ_TABLE_EXACT) {
-        // the hash is a bijection of the key for 4-byte keys only
-        if (d->key_bytes != 4 || p->table_capacity < 64 || p->table_capacity > MAX_BUCKET_CAP) return PJ_ERR_INVALID;
+        if (p->table_capacity < 64 || p->table_capacity > MAX_BUCKET_CAP) return PJ_ERR_INVALID;
         const int nb = table_nb_log2(d->n_build, p);
-        if (nb > 20 || join_smem(4, PJ_TABLE_EXACT, p->table_capacity, nb) > smem_limit()) return PJ_ERR_INVALID;
+        if (nb > 20 || join_smem(d->key_bytes, PJ_TABLE_EXACT, p->table_capacity, nb) > smem_limit())
+            return PJ_ERR_INVALID;
     } else if (p->table_capacity < 64 || p->table_capacity > max_table_capacity(d->key_bytes, p->table_mode)) {
         return PJ_ERR_INVALID;
     }
@@ -720,10 +721,7 @@ pj_status launch_join(const JoinArgs& a, int table_mode, bool unique, bool hash_
 {
     if (table_mode == PJ_TABLE_BUCKET) return launch_join_tab<K, TABLE_BUCKET>(a, unique, hash_split, false, st);
     if (table_mode == PJ_TABLE_COMPACT) return launch_join_tab<K, TABLE_COMPACT>(a, unique, hash_split, false, st);
-    if (table_mode == PJ_TABLE_EXACT) {
-        if constexpr (sizeof(K) == 4) return launch_join_tab<K, TABLE_EXACT>(a, unique, hash_split, false, st);
-        return PJ_ERR_INVALID;  // check_plan admits EXACT tables for 4-byte keys only
-    }
+    if (table_mode == PJ_TABLE_EXACT) return launch_join_tab<K, TABLE_EXACT>(a, unique, hash_split, false, st);
     return launch_join_tab<K, TABLE_OPEN>(a, unique, hash_split, slot_ref, st);
 }
 
@@ -1084,11 +1082,11 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     p->bits1 = bits;
     p->wc_tuples = pick_w(bits);
     if (p->wc_tuples == 0) p->wc_tuples = d->key_bytes == 4 ? 4 : 8;
-    if (d->key_bytes == 4 && p->table_mode == PJ_TABLE_COMPACT) {
+    if (p->table_mode == PJ_TABLE_COMPACT) {
         // EXACT tables (no build-tuple loads) where the expected largest
         // hashed partition (mean + 4 standard deviations) fits one
         const double m = static_cast<double>(d->n_build) / static_cast<double>(int64_t(1) << bits);
-        const int cap_e = exact_table_capacity(exact_row_bits(d->n_build) - bits);
+        const int cap_e = exact_table_capacity(d->key_bytes, exact_row_bits(d->n_build) - bits);
         if (cap_e > 0 && m + 4.0 * std::sqrt(m) + 1.0 <= cap_e) {
             p->table_mode = PJ_TABLE_EXACT;
             p->table_capacity = cap_e;
@@ -1386,11 +1384,14 @@ pj_status pj_plan_exact(const pj_join_desc* d, void* ws, size_t ws_bytes, pj_pla
         p.table_mode = PJ_TABLE_BUCKET;
         p.table_capacity = max_table_capacity(d->key_bytes, PJ_TABLE_BUCKET);
     }
-    // 4-byte keys: EXACT tables instead of COMPACT ones (no build-tuple
-    // loads) where hash digits keep the largest partition within one
+    // EXACT tables instead of COMPACT ones (no build-tuple loads) where hash
+    // digits keep the largest partition within one -- unless the heavy-key
+    // path takes most probe rows: then the join has few lookups to save and
+    // the hash digits' histogram costs more (2^26 x 2^28 int64 at Zipf 1.5:
+    // 5.06 ms with EXACT tables, 4.84 ms without)
     int64_t mx_plan = mx;
-    if (d->key_bytes == 4 && p.passes == 1 && p.table_mode == PJ_TABLE_COMPACT) {
-        const int cap_e = exact_table_capacity(exact_row_bits(d->n_build) - p.bits1);
+    if (p.passes == 1 && p.table_mode == PJ_TABLE_COMPACT && p.n_heavy == 0) {
+        const int cap_e = exact_table_capacity(d->key_bytes, exact_row_bits(d->n_build) - p.bits1);
         if (cap_e > 0 && hash_max <= cap_e) {
             p.table_mode = PJ_TABLE_EXACT;
             p.digit_mode = PJ_DIGIT_HASH;

@@ -228,6 +228,39 @@ template <> struct TupleView<int64_t> {
     }
 };
 
+// Entry of an EXACT table: the tag (hash bits above the bucket bits) << R |
+// build row, R = row bits.  A 4-byte key is its MurmurHash3 value (a
+// bijection), so the tag, the bucket and the partition's hash digits fix the
+// key.  For an 8-byte key MurmurHash3_x86_32 maps the high word to the hash
+// bijectively for each low word (the second block's mixing, rotation,
+// multiply-add, length xor and fmix32 are all invertible), so (low word,
+// hash) fixes the key: the entry keeps the low word beside the tag.
+template <typename K> struct ExactEntry;
+template <> struct ExactEntry<int32_t> {
+    static constexpr int BYTES = 4;
+    __device__ __forceinline__ static void put(uint8_t* t, int i, uint32_t tag, uint32_t) { reinterpret_cast<uint32_t*>(t)[i] = tag; }
+    __device__ __forceinline__ static uint32_t get(const uint8_t* t, int i, uint32_t& key_lo)
+    {
+        key_lo = 0u;
+        return reinterpret_cast<const uint32_t*>(t)[i];
+    }
+    __device__ __forceinline__ static uint32_t key_lo(uint32_t) { return 0u; }
+};
+template <> struct ExactEntry<int64_t> {
+    static constexpr int BYTES = 8;
+    __device__ __forceinline__ static void put(uint8_t* t, int i, uint32_t tag, uint32_t lo)
+    {
+        reinterpret_cast<uint2*>(t)[i] = make_uint2(lo, tag);
+    }
+    __device__ __forceinline__ static uint32_t get(const uint8_t* t, int i, uint32_t& key_lo)
+    {
+        const uint2 v = reinterpret_cast<const uint2*>(t)[i];
+        key_lo = v.x;
+        return v.y;
+    }
+    __device__ __forceinline__ static uint32_t key_lo(unsigned long long k) { return static_cast<uint32_t>(k); }
+};
+
 // Entry of a BUCKET table.
 template <typename K> struct Entry;
 template <> struct Entry<int32_t> {
@@ -304,7 +337,8 @@ struct JoinSmem {
     __host__ __device__ static size_t entries_bytes(int cap)
     {
         const size_t e = TABLE == TABLE_OPEN                                    ? (sizeof(K) == 4 ? 8 : 12)
-                         : (TABLE == TABLE_COMPACT || TABLE == TABLE_EXACT) ? 4
+                         : TABLE == TABLE_EXACT                                ? ExactEntry<K>::BYTES
+                         : TABLE == TABLE_COMPACT                              ? 4
                                                                             : Entry<K>::BYTES;
         return (static_cast<size_t>(cap) * e + 127) & ~size_t(127);
     }
@@ -581,7 +615,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             if constexpr (TABLE == TABLE_COMPACT)
                                 ctab[pos] = (finger_of(h[u]) << 16) | static_cast<uint32_t>(i0 + u * THREADS - b_lo);
                             else if constexpr (TABLE == TABLE_EXACT)
-                                ctab[pos] = (xfinger_of(h[u]) << a.row_bits) | static_cast<uint32_t>(r[u]);
+                                ExactEntry<K>::put(table, pos, (xfinger_of(h[u]) << a.row_bits) | static_cast<uint32_t>(r[u]),
+                                                   ExactEntry<K>::key_lo(k[u]));
                             else
                                 E::put(table, pos, k[u], r[u]);
                         }
@@ -690,11 +725,12 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         }
                         if (!found || UNIQUE) live_u = false;
                     } else if constexpr (TABLE == TABLE_EXACT) {
-                        const uint32_t fq = xfinger_of(h[u]);
+                        const uint32_t fq = xfinger_of(h[u]), klo = ExactEntry<K>::key_lo(k[u]);
                         while (at_u < end_u) {
-                            const uint32_t e = ctab[at_u];
+                            uint32_t elo;
+                            const uint32_t e = ExactEntry<K>::get(table, at_u, elo);
                             ++at_u;
-                            if ((e >> a.row_bits) == fq) {  // the whole hash, so the key, is equal
+                            if ((e >> a.row_bits) == fq && elo == klo) {  // the key is equal
                                 found = true;
                                 brow_u = e & x_rmask;
                                 break;
@@ -849,9 +885,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
                             if (live[u]) {
-                                const uint32_t e = ctab[at[u]];
+                                uint32_t elo;
+                                const uint32_t e = ExactEntry<K>::get(table, at[u], elo);
                                 ++at[u];
-                                if ((e >> a.row_bits) == fq[u]) {
+                                if ((e >> a.row_bits) == fq[u] && elo == ExactEntry<K>::key_lo(k[u])) {
                                     emit[u] = true;
                                     brow[u] = e & x_rmask;
                                     live[u] = false;

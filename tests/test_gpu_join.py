@@ -263,19 +263,24 @@ def test_join_compact_fingerprint_collisions(dtype, unique):
     assert pairs_equal(build, probe, br, pr, unique)
 
 
+@pytest.mark.parametrize("dtype", [np.int32, np.int64])
 @pytest.mark.parametrize("unique", [True, False])
 @pytest.mark.parametrize("split", [SPLIT_HASH, SPLIT_POSITION])
 @pytest.mark.parametrize("n_build", [4096, 4097, 300007])
-def test_join_exact_tables_match_oracle(unique, split, n_build):
+def test_join_exact_tables_match_oracle(dtype, unique, split, n_build):
     # EXACT entries hold the build row in the low bits (12, 13 and 19 row
-    # bits here) and the hash bits above the bucket bits; small tables force
-    # several pieces per partition
+    # bits here) and the hash bits above the bucket bits (8-byte keys: and
+    # the key's low word); small tables force several pieces per partition
     rng = np.random.default_rng(n_build)
-    b = rng.permutation(np.arange(1, 3 * n_build, 3, dtype=np.int64))[:n_build].astype(np.int32)
+    b = rng.permutation(np.arange(1, 3 * n_build, 3, dtype=np.int64))[:n_build]
+    if dtype == np.int64:
+        b = b * 0x100000001 + (b % 7) * (1 << 40)   # high words matter
+    b = b.astype(dtype)
     if not unique:
         b[: n_build // 10] = b[n_build // 10: 2 * (n_build // 10)]
-    p = np.concatenate([rng.choice(b, 2 * n_build), rng.integers(-(1 << 31), (1 << 31) - 1, n_build)]).astype(np.int32)
-    plan = api.plan_default(n_build, p.shape[0], 4, unique)
+    info = np.iinfo(dtype)
+    p = np.concatenate([rng.choice(b, 2 * n_build), rng.integers(info.min, info.max, n_build)]).astype(dtype)
+    plan = api.plan_default(n_build, p.shape[0], np.dtype(dtype).itemsize, unique)
     plan.table_mode, plan.digit_mode, plan.split_mode = TABLE_EXACT, DIGIT_HASH, split
     plan.bits1 = 4
     plan.wc_tuples = 4
@@ -333,17 +338,30 @@ def test_join_exact_tables_hash_twins():
     assert pairs_equal(build, probe, br, pr)
 
 
-def test_join_exact_tables_planned_for_large_int32_builds():
+def test_join_exact_tables_int64_same_low_words():
+    # 8-byte keys that share their low word and differ only in the high
+    # word: the entry's low word and hash bits still tell them apart
+    lo = np.arange(1, 2001, dtype=np.int64)
+    keys = np.concatenate([lo + (h << 32) for h in range(1, 41)])      # 40 keys per low word
+    rng = np.random.default_rng(38)
+    rng.shuffle(keys)
+    build = keys[::2]
+    probe = np.concatenate([keys, keys[:5000]])
+    plan = api.plan_default(build.shape[0], probe.shape[0], 8)
+    plan.table_mode, plan.digit_mode, plan.bits1, plan.wc_tuples = TABLE_EXACT, DIGIT_HASH, 3, 2
+    plan.table_capacity = 4096
+    br, pr = run(build, probe, True, plan)
+    assert pairs_equal(build, probe, br, pr)
+
+
+def test_join_exact_tables_planned_where_they_fit():
     assert api.plan_default(1 << 27, 1 << 27, 4).table_mode == TABLE_EXACT
+    assert api.plan_default(1 << 26, 1 << 28, 8).table_mode == TABLE_EXACT
+    # 32 K-tuple partitions of 8-byte keys exceed an EXACT table's ~22 K
     assert api.plan_default(1 << 27, 1 << 27, 8).table_mode == TABLE_COMPACT
 
 
 def test_join_exact_tables_rejected_where_inexact():
-    b = np.arange(1, 1000, dtype=np.int64)
-    plan = api.plan_default(b.shape[0], b.shape[0], 8)
-    plan.table_mode, plan.digit_mode, plan.table_capacity = TABLE_EXACT, DIGIT_HASH, 1024
-    with pytest.raises(PJError):             # 8-byte keys: the hash is not a bijection
-        run(b, b, True, plan)
     b32 = np.arange(1, 1 << 20, dtype=np.int32)
     plan = api.plan_default(b32.shape[0], b32.shape[0], 4)
     plan.table_mode, plan.digit_mode, plan.bits1, plan.wc_tuples = TABLE_EXACT, DIGIT_RAW, 0, 4
