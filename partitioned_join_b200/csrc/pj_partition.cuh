@@ -131,15 +131,25 @@ __global__ void __launch_bounds__(HIST_THREADS) hist_keys_kernel(const K* __rest
     };
     constexpr int STEP = HIST_THREADS * VN * HIST_UNROLL;
     int64_t base = s_lo;
+    // the next step's vectors load while this step's keys are counted
+    K v[HIST_UNROLL][VN];
+    auto load_step = [&](int64_t at) {
+#pragma unroll
+        for (int u = 0; u < HIST_UNROLL; ++u)
+            load_vec16<K>(keys + at + (static_cast<int64_t>(u) * HIST_THREADS + threadIdx.x) * VN, v[u]);
+    };
+    if (base + STEP <= s_hi) load_step(base);
     for (; base + STEP <= s_hi; base += STEP) {
-        K v[HIST_UNROLL][VN];
-#pragma unroll
-        for (int u = 0; u < HIST_UNROLL; ++u)
-            load_vec16<K>(keys + base + (static_cast<int64_t>(u) * HIST_THREADS + threadIdx.x) * VN, v[u]);
+        K c[HIST_UNROLL][VN];
 #pragma unroll
         for (int u = 0; u < HIST_UNROLL; ++u)
 #pragma unroll
-            for (int e = 0; e < VN; ++e) count(v[u][e]);
+            for (int e = 0; e < VN; ++e) c[u][e] = v[u][e];
+        if (base + 2 * STEP <= s_hi) load_step(base + STEP);
+#pragma unroll
+        for (int u = 0; u < HIST_UNROLL; ++u)
+#pragma unroll
+            for (int e = 0; e < VN; ++e) count(c[u][e]);
     }
     for (int64_t i = base + threadIdx.x; i < s_hi; i += HIST_THREADS) count(keys[i]);
     if constexpr (HEAVY) {
