@@ -115,7 +115,8 @@ constexpr int32_t PAD_ROW = -1;
 template <int THREADS>
 __device__ __forceinline__ void scan_u16_pairs(uint32_t* w, int nwords, uint32_t* s_warp)
 {
-    const int per = (nwords + THREADS - 1) / THREADS;
+    // an odd run length: the lanes of a warp then walk 32 different banks
+    const int per = ((nwords + THREADS - 1) / THREADS) | 1;
     const int a = threadIdx.x * per;
     const int b = a + per < nwords ? a + per : nwords;
     uint32_t sum = 0;
