@@ -9,7 +9,7 @@ the library's own kernels (pj_mlp_forward / pj_mlp_backward /
 pj_mlp_mse_grad / pj_mlp_adam) on timings that the plain method generates
 over a seeded synthetic sweep.  The exact-histogram planner (pj_plan_exact)
 is both the fallback -- a learned choice whose table overflows on the device
-is rerun with it -- and the judge: the sweep times it beside every
+is rerun with it -- and the yardstick: the sweep times it beside every
 candidate.  The network picks a schedule, never a result.
 
     python -m partitioned_join_b200.planner --train --workloads 400 --out weights.npz
