@@ -1053,7 +1053,9 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 // segments (>= total), their prefix sums; *count = total.
 // seg layout: [0] = n_holes, [1] = n_movers, [2] = moves; then
 // hole (start, prefix) pairs, then mover (start, prefix) pairs.
-__global__ void __launch_bounds__(1024) join_fixup_plan_kernel(const int64_t* __restrict__ cta_q,
+constexpr int MAX_FIXUP_CTAS = 1024;  // join CTAs one fix-up plan covers: one thread (and gap) each
+
+__global__ void __launch_bounds__(MAX_FIXUP_CTAS) join_fixup_plan_kernel(const int64_t* __restrict__ cta_q,
                                                                const int64_t* __restrict__ cta_last, int32_t n_cta,
                                                                unsigned long long* count,
                                                                const unsigned long long* __restrict__ base_count,
@@ -1062,8 +1064,12 @@ __global__ void __launch_bounds__(1024) join_fixup_plan_kernel(const int64_t* __
                                                                uint32_t* __restrict__ status)
 {
     __shared__ long long s_sum;
-    __shared__ long long g_start[1024], g_len[1024];
+    __shared__ long long g_start[MAX_FIXUP_CTAS], g_len[MAX_FIXUP_CTAS];
     __shared__ int s_ng;
+    if (n_cta > static_cast<int>(blockDim.x)) {  // gaps of CTAs past the block would stay unfilled
+        if (threadIdx.x == 0) raise_status(status, ST_INTERNAL);
+        return;
+    }
     if (threadIdx.x == 0) {
         s_sum = 0;
         s_ng = 0;

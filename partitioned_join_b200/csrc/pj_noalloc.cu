@@ -78,8 +78,11 @@ extern "C" pj_status pj_inner_join_noalloc(const pj_join_desc* desc, const pj_pl
     void* ws = nullptr;
     if ((s = scratch_address(&ws)) != PJ_OK) return s;
     s = pj_inner_join(desc, plan, out, ws, PJ_NOALLOC_SCRATCH_BYTES, stream);
-    // pj_check waits for the join and clears the status word even when the
-    // launch itself failed part-way, so the next call starts clean.
+    // Arguments rejected before any launch leave nothing on the device to
+    // wait for.  After a launch (or a launch that failed part-way), pj_check
+    // waits for the join and clears the status word, so the next call starts
+    // clean.
+    if (s != PJ_OK && s != PJ_ERR_CUDA) return s;
     const pj_status device_status = pj_check(ws, stream);
     return s != PJ_OK ? s : device_status;
 }
