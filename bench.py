@@ -60,6 +60,7 @@ def parse_args():
                     help="build and probe rows of the bounded CPU sample (log2)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="--impl reference: skip the reference's GPU path")
     ap.add_argument("--plan", type=str, default="", help="JSON overrides of pj_plan fields")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--default-plan", action="store_true", help="plan from sizes only (no histogram)")
@@ -95,6 +96,52 @@ def cpu_sample(log2n, match_rate, seed):
     from partitioned_join_b200 import datagen
     n = 1 << log2n
     return datagen.config2(seed=seed, n_build=n, n_probe=n, match_rate=match_rate)
+
+
+def workload_config(args, world):
+    """The workload's description, shared by both arms' JSON lines."""
+    if args.workload == "cfg2":
+        w = (f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2): build = seeded permutation of "
+             f"0..2^{args.log2_build}-1, probe {args.match_rate:.0%} uniform hits, the rest above the build keys")
+    else:
+        w = (f"2^{args.log2_build}x2^{args.log2_probe} int64 inner join (cfg3): unique random build keys, probe keys "
+             f"Zipf({args.zipf}) over a seeded rank order")
+    return {"workload": w, "build_rows": 1 << args.log2_build, "probe_rows": 1 << args.log2_probe,
+            "unique_build_keys": True, "match_rate": args.match_rate if args.workload == "cfg2" else 1.0,
+            "l2": "inputs (1 GiB or more) larger than L2, no flush", "parallelism": f"replicas x{world}"}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def verify_pairs_device(build, probe, build_row, probe_row, n, expected):
+    """Pair-level check of a unique-build-key join on the device: every
+    output pair joins equal keys, both row ids are in range, no probe row
+    appears twice, and the pair count equals the number of probe rows the
+    generator made to match.  With unique build keys each matching probe row
+    has exactly one partner, so these together make the output the same
+    multiset as inner_join_cpu's (inner_join_cpu.hpp:24-107)."""
+    import torch
+    br = build_row[:n].long()
+    pr = probe_row[:n].long()
+    in_range = bool(((br >= 0) & (br < build.numel()) & (pr >= 0) & (pr < probe.numel())).all().item())
+    keys_equal = in_range and bool((build[br] == probe[pr]).all().item())
+    seen = torch.zeros(probe.numel(), dtype=torch.int32, device=probe.device)
+    if in_range:
+        seen.index_add_(0, pr, torch.ones_like(pr, dtype=torch.int32))
+    distinct = in_range and int(seen.max().item() if n else 0) <= 1
+    del seen, br, pr
+    res = {"pairs_checked": int(n), "rows_in_range": in_range, "keys_equal": keys_equal,
+           "probe_rows_distinct": distinct, "count_equals_generator": int(n) == int(expected)}
+    res["ok"] = all(v for k, v in res.items() if k != "pairs_checked")
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -214,14 +261,49 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "ms_per_step_median": 1e3 * statistics.median(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2), "
-                               f"CPU sample 2^{args.cpu_sample_log2}x2^{args.cpu_sample_log2}",
-                   "build_rows": 1 << args.cpu_sample_log2, "probe_rows": 1 << args.cpu_sample_log2},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "config": workload_config(args, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "cpu_model": cpu_model(),
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu(args)
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu(args):
+    """The reference's own GPU path (main.cu:762-892), compiled unchanged for
+    sm_100a into oracle/_ref, on the full workload: -R -n 256 -N 512 -u -V
+    (two radix passes, the largest partition counts its 96 000-byte table
+    cap admits at 2^27 rows, partitioned_join.cuh:198-206,324).  Its inputs
+    are host columns from the numpy generator with the same recipe; the
+    stage times are the reference's own cudaEvent timers around each stage
+    (main.cu:769-896), copies and allocations excluded."""
+    import numpy as np
+
+    from oracle import oracle
+    from partitioned_join_b200 import datagen
+    if args.workload != "cfg2" or not oracle.ref_gpu_available(4):
+        return {"unavailable": "reference GPU library not built (oracle/build_ref.sh) or workload not cfg2"}
+    n_b, n_p = 1 << args.log2_build, 1 << args.log2_probe
+    b, p = datagen.config2(seed=args.seed, n_build=n_b, n_probe=n_p, match_rate=args.match_rate)
+    expected = int(np.count_nonzero(p <= n_b))
+    p1, p2, factor = 256, 512, 3.0
+    runs = []
+    count_ok = True
+    for k in range(4):
+        keys, rows, ms = oracle.ref_gpu_partitioned_join(b, p, True, True, True, p1, p2, factor, False, capacity=n_p)
+        count_ok &= keys.shape[0] == expected
+        if k > 0:  # the first run is a warm-up
+            runs.append([float(x) for x in ms])
+    names = ["combined_histogram", "partition_pass1", "partition_pass2", "skew_handler", "join", "total"]
+    med = {n: statistics.median(r[i] for r in runs) for i, n in enumerate(names)}
+    return {"flags": f"-R -n {p1} -N {p2} -f {factor} -u -V", "build_rows": n_b, "probe_rows": n_p,
+            "runs": len(runs), "stages_ms_median": med, "ms_per_join": med["total"],
+            "tuples_per_s": (n_b + n_p) / (med["total"] / 1e3), "count_equals_generator": bool(count_ok),
+            "timer": "the reference's own stage events (main.cu:769-896), median of 3 runs after 1 warm-up"}
 
 
 def run_ours(args, rank, world, local):
@@ -245,23 +327,34 @@ def run_ours(args, rank, world, local):
         build, probe, expected = api.generate_tables(n_b, n_p, torch.int64, (1 << 62) - 1, 1.0, True, args.zipf, seed,
                                                      device)
     kb = build.element_size()
-    # the exact-histogram planner picks the digit source (and split) from the data
-    plan = api.plan_exact(build, probe, True) if not args.default_plan else api.plan_default(n_b, n_p, kb, True)
+    # Planning belongs to the timed step.  The size-only planner runs inside
+    # every pj_inner_join call (a null plan); where the exact-histogram
+    # planner (which reads the keys) would choose differently, its plan is
+    # made once before the timed region and the line says so.
+    plan_sizes = api.plan_default(n_b, n_p, kb, True)
+    plan_hist = api.plan_exact(build, probe, True)
+    same = plan_sizes.as_dict() == plan_hist.as_dict()
+    plan = plan_sizes if (same or args.default_plan) else plan_hist
     if args.plan:
         for k, v in json.loads(args.plan).items():
             setattr(plan, k, v)
-    j = api.Joiner(build, probe, True, plan, capacity=n_p)
+    per_call = (same or args.default_plan) and not args.plan
+    j = api.Joiner(build, probe, True, plan, capacity=n_p, plan_per_call=per_call)
+    plan_note = ("pj_plan_default inside every timed pj_inner_join call (a null plan); it equals "
+                 "pj_plan_exact's plan for these inputs" if per_call and same else
+                 "pj_plan_default inside every timed pj_inner_join call (a null plan)" if per_call else
+                 "plan made once before the timed region (pj_plan_exact or --plan)")
     stream = torch.cuda.current_stream()
 
-    # warm-up, and a correctness check of the count
+    # warm-up, then a pair-level check of the warm-up join's output
     for _ in range(max(args.warmup, 1)):
         j.launch()
     st = j.status()
     _lib.check(st, "warm-up join")
     got = int(j.count.item())
-    verified = got == expected
-    if not verified:
-        raise SystemExit(f"bench: join produced {got} pairs, expected {expected}")
+    verified = verify_pairs_device(build, probe, j.build_row, j.probe_row, got, expected)
+    if not verified["ok"]:
+        raise SystemExit(f"bench: join output failed the pair check: {verified} (expected {expected} pairs)")
 
     # timed region: K steps with per-stage events
     n_st = len(_lib.STAGES)
@@ -289,12 +382,17 @@ def run_ours(args, rank, world, local):
         for i, name in enumerate(_lib.STAGES[:-1]):
             stage_ms[name] += row[i].elapsed_time(row[i + 1]) / args.steps
     step_ms = ms / args.steps
+    step_median = replicas.max_over_ranks(statistics.median(row[0].elapsed_time(row[-1]) for row in ev), device)
+    # the last timed join's output, checked pair by pair like the warm-up's
+    verified_last = verify_pairs_device(build, probe, j.build_row, j.probe_row, int(j.count.item()), expected)
+    if not verified_last["ok"]:
+        raise SystemExit(f"bench: timed join output failed the pair check: {verified_last}")
     tuples_all = replicas.sum_over_ranks((n_b + n_p) * args.steps, device)
     value = replicas.whole_job_rate(tuples_all, ms)
 
     # roofline: the dominant kernel and the whole join
     peak, peak_kind = measured_peak_gbs()
-    tb = 8 if kb == 4 else 12  # partitioned tuple bytes
+    tb = 8 if kb == 4 else 16  # partitioned tuple bytes: {hash, row} or {key_lo, key_hi, hash, row}
     alg = {
         "build_hist": n_b * kb, "probe_hist": n_p * kb,
         "build_scatter": n_b * (kb + tb), "probe_scatter": n_p * (kb + tb),
@@ -315,15 +413,11 @@ def run_ours(args, rank, world, local):
         "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32" if kb == 4 else "int64", "data": "synthetic",
-        "config": {"workload": (f"2^{args.log2_build}x2^{args.log2_probe} int32 inner join (cfg2): build = seeded "
-                                f"permutation of 0..2^{args.log2_build}-1, probe {args.match_rate:.0%} uniform hits, "
-                                f"the rest above the build keys (generated on the device)")
-                   if args.workload == "cfg2" else
-                   (f"2^{args.log2_build}x2^{args.log2_probe} int64 inner join (cfg3): unique random build keys, "
-                    f"probe keys Zipf({args.zipf}) over a seeded rank order (generated on the device)"),
-                   "build_rows": n_b, "probe_rows": n_p, "output_pairs": expected, "unique_build_keys": True,
-                   "l2": "inputs (1 GiB) larger than L2, no flush", "parallelism": f"replicas x{world}",
-                   "plan": plan.as_dict()},
+        "config": workload_config(args, world),
+        "inputs": "generated on the device by pj_generate_tables (seeded)",
+        "output_pairs": expected,
+        "plan": plan.as_dict(), "planning": plan_note,
+        "ms_per_step_median": step_median,
         "clocks": clk,
         "gpu_launches": LAUNCHES_PER_JOIN * args.steps,
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
@@ -332,7 +426,7 @@ def run_ours(args, rank, world, local):
                      "traffic": traffic, "algorithmic_bytes_per_launch": alg[dom]},
         "roofline_join": {"algorithmic_bytes": b_alg, "achieved": join_gbs, "peak": peak, "unit": "GB/s",
                           "frac": join_gbs / peak, "frac_keys_only": (b_keys / (step_ms / 1e3) / 1e9) / peak},
-        "verified": verified,
+        "verified": {"warmup_join": verified, "last_timed_join": verified_last},
     }
 
     if not args.no_e2e:
@@ -357,7 +451,7 @@ def e2e_measure(args, j, build, probe, stream):
     from partitioned_join_b200 import api
 
     cap = j.capacity
-    js = [j, api.Joiner(build.clone(), probe.clone(), True, j.plan, capacity=cap)]
+    js = [j, api.Joiner(build.clone(), probe.clone(), True, j.plan, capacity=cap, plan_per_call=j.plan_per_call)]
     hb = build.cpu().pin_memory()
     hp = probe.cpu().pin_memory()
     ob = [torch.empty(cap, dtype=torch.int32).pin_memory() for _ in range(2)]
@@ -441,6 +535,7 @@ def cpu_baseline(args):
         oracle.inner_join(b, p, True)
         secs, kind, cores = time.perf_counter() - t0, "port", 1
     return {"value": (b.shape[0] + p.shape[0]) / secs, "unit": UNIT, "cores": cores, "kind": kind,
+            "cpu_model": cpu_model(),
             "sample": f"2^{args.cpu_sample_log2} x 2^{args.cpu_sample_log2} rows of the cfg2 generator, "
                       f"inner_join_cpu's own timer (build + probe)"}
 
@@ -504,22 +599,30 @@ def run_batch(args, rank, world, local):
             _lib.check(L.pj_inner_join(ctypes.byref(d), ctypes.byref(pl), ctypes.byref(o),
                                        ctypes.c_void_p(ws.data_ptr()), ws_bytes, api._stream_ptr(None)))
 
+    def verify_all(brs, prs, cnts):
+        """Pair-level check of every join of the batch (verify_pairs_device)."""
+        cnts = cnts.cpu().tolist()
+        bad = [i for i, (b, p) in enumerate(pairs)
+               if not verify_pairs_device(b, p, brs[i], prs[i], cnts[i], expected[i])["ok"]]
+        return {"joins_checked": len(pairs), "pairs_checked": int(sum(cnts)), "failed_joins": bad[:8],
+                "ok": not bad}
+
     steps = max(1, min(args.steps, 5))
     plain_ms = timed(plain, steps)
     _lib.check(L.pj_check(ctypes.c_void_p(ws.data_ptr()), None))
-    plain_ok = counts.cpu().tolist() == expected
+    plain_ok = verify_all(keep[0::2], keep[1::2], counts)
 
     bj = api.BatchJoiner(pairs)
     default_cfg = bj.config.as_dict()
     batch_ms = timed(bj.launch, steps)
     bj.check()
-    batch_ok = bj.count.cpu().tolist() == expected
+    batch_ok = verify_all(bj.build_row, bj.probe_row, bj.count)
     tuned_ms_est = bj.autotune()
     tuned_ms = timed(bj.launch, steps)
     g = bj.graph()
     graph_ms = timed(g.replay, steps)
     bj.check()
-    graph_ok = bj.count.cpu().tolist() == expected
+    graph_ok = verify_all(bj.build_row, bj.probe_row, bj.count)
     best_ms = min(batch_ms, tuned_ms, graph_ms)
     line = {
         "metric": "tuples/s, 512-join uneven batch (cfg5)", "value": tuples / (best_ms / 1e3), "unit": UNIT,

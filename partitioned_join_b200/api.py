@@ -115,13 +115,21 @@ class Joiner:
     (sizes, plan), so repeated joins allocate nothing (bench and batch use)."""
 
     def __init__(self, build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_keys: bool = True,
-                 plan: Optional[Plan] = None, capacity: Optional[int] = None):
+                 plan: Optional[Plan] = None, capacity: Optional[int] = None, plan_per_call: bool = False):
+        """plan_per_call: every launch passes a null plan, so the library
+        plans from the sizes (pj_plan_default) inside each call; `plan` must
+        then be that same default plan (the workspace is sized for it)."""
+        self.plan_per_call = plan_per_call
         self.build_keys = _keys(build_keys, "build_keys")
         self.probe_keys = _keys(probe_keys, "probe_keys")
         self.unique = unique_build_keys
         self.desc = make_desc(self.build_keys, self.probe_keys, unique_build_keys)
         self.plan = plan if plan is not None else plan_default(self.desc.n_build, self.desc.n_probe,
                                                                self.desc.key_bytes, unique_build_keys)
+        if plan_per_call:
+            default = plan_default(self.desc.n_build, self.desc.n_probe, self.desc.key_bytes, unique_build_keys)
+            if default.as_dict() != self.plan.as_dict():
+                raise ValueError("plan_per_call needs the size-only default plan")
         dev = self.build_keys.device
         self.ws_bytes = workspace_size(self.desc, self.plan)
         self.ws = alloc_workspace(self.ws_bytes, dev)
@@ -142,9 +150,12 @@ class Joiner:
 
     def launch(self, stream=None) -> None:
         """Enqueue the join on the stream (asynchronous)."""
-        check(lib().pj_inner_join(ctypes.byref(self.desc), ctypes.byref(self.plan), ctypes.byref(self._out()),
+        check(lib().pj_inner_join(ctypes.byref(self.desc), self._plan_arg(), ctypes.byref(self._out()),
                                   ctypes.c_void_p(self.ws.data_ptr()), self.ws_bytes, _stream_ptr(stream)),
               "pj_inner_join")
+
+    def _plan_arg(self):
+        return None if self.plan_per_call else ctypes.byref(self.plan)
 
     def _out(self) -> Output:
         out = Output()
@@ -159,14 +170,14 @@ class Joiner:
         (len(events) == len(_lib.STAGES)); the events must already exist
         (recorded once)."""
         arr = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
-        check(lib().pj_inner_join_events(ctypes.byref(self.desc), ctypes.byref(self.plan), ctypes.byref(self._out()),
+        check(lib().pj_inner_join_events(ctypes.byref(self.desc), self._plan_arg(), ctypes.byref(self._out()),
                                          ctypes.c_void_p(self.ws.data_ptr()), self.ws_bytes, _stream_ptr(stream), arr),
               "pj_inner_join_events")
 
     def launch_timed(self, stream=None):
         """Run once with per-stage timers (synchronising); returns {stage: ms}."""
         ms = (ctypes.c_float * len(_lib.STAGES))()
-        check(lib().pj_inner_join_timed(ctypes.byref(self.desc), ctypes.byref(self.plan), ctypes.byref(self._out()),
+        check(lib().pj_inner_join_timed(ctypes.byref(self.desc), self._plan_arg(), ctypes.byref(self._out()),
                                         ctypes.c_void_p(self.ws.data_ptr()), self.ws_bytes, _stream_ptr(stream), ms),
               "pj_inner_join_timed")
         return dict(zip(_lib.STAGES, list(ms)))

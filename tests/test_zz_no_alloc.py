@@ -3,7 +3,9 @@
 Collected last on purpose: the built-in workspace is per-process state, and
 these tests must pass both alone and after every other test has run joins on
 the same device.  Two joins in a row on the built-in workspace must each
-give exactly the pairs that pj_inner_join gives with a caller workspace."""
+give exactly the oracle's pairs (oracle.inner_join, the restatement of the
+reference's inner_join_cpu), which are also the pairs pj_inner_join gives
+with a caller workspace."""
 import ctypes
 
 import numpy as np
@@ -46,7 +48,10 @@ def test_noalloc_two_calls_match_pj_inner_join():
         pt = torch.from_numpy(p).to(dev)
         assert api.workspace_size(api.make_desc(bt, pt)) <= _lib.NOALLOC_SCRATCH_BYTES
         inputs.append((bt, pt))
-        expected.append(_sorted(*api.partitioned_join(bt, pt)))
+        eb, ep = oracle.inner_join(b, p, True)
+        exp = oracle.sorted_pairs(eb, ep)
+        assert np.array_equal(_sorted(*api.partitioned_join(bt, pt)), exp)
+        expected.append(exp)
     # two calls in a row on the built-in workspace
     got = [api.inner_join_noalloc(bt, pt, capacity=pt.numel()) for bt, pt in inputs]
     torch.cuda.synchronize()
