@@ -160,6 +160,18 @@ const char* pj_version(void);
  * B200 shared-memory limits. */
 pj_status pj_plan_default(const pj_join_desc* desc, pj_plan* plan);
 
+/* The reference's own partitioning flags as a plan: -n partitions_1,
+ * -R -N partitions_2 (0: one pass) and -f factor (main.cu:239-251; pass one
+ * main.cu:804-810, pass two :826-852, the factor :867).  Pass 1 takes raw
+ * key bits as its digit (partition_kernels.cuh:168), pass 2 the top hash
+ * bits; partitions are cut into build pieces of at most
+ * ceil(factor * n_build / partitions) rows by position, as
+ * handle_skewed_data does (skewed_data_handler.cuh:59-91), each piece one
+ * BUCKET table.  PJ_ERR_INVALID for partition counts that are not powers of
+ * two, a non-positive factor, or a fan-out one scatter pass cannot make. */
+pj_status pj_plan_radix(const pj_join_desc* desc, int32_t partitions_1, int32_t partitions_2, float factor,
+                        pj_plan* plan);
+
 /* Bytes of device workspace that pj_inner_join / pj_join_count need for
  * this join and plan (plan NULL: the default plan).  The workspace must be
  * 256-byte aligned. */
@@ -187,16 +199,18 @@ pj_status pj_join_count(const pj_join_desc* desc, const pj_plan* plan, int64_t* 
 /* Stage timers of pj_inner_join, like the reference's per-stage cudaEvent
  * timers and CSV columns (main.cu:769-896, 918-948). */
 enum {
-    PJ_STAGE_BUILD_HIST = 0,
-    PJ_STAGE_BUILD_SCAN = 1,
-    PJ_STAGE_BUILD_SCATTER = 2,
-    PJ_STAGE_PROBE_HIST = 3,
-    PJ_STAGE_PROBE_SCAN = 4,
-    PJ_STAGE_PROBE_SCATTER = 5,
-    PJ_STAGE_JOIN_PLAN = 6,  /* work split: the reference's handle_skewed_data */
-    PJ_STAGE_JOIN = 7,
-    PJ_STAGE_TOTAL = 8,
-    PJ_NUM_STAGES = 9
+    PJ_STAGE_BUILD_HIST = 0,     /* pass one of the build side: histogram, */
+    PJ_STAGE_BUILD_SCAN = 1,     /*   scan, */
+    PJ_STAGE_BUILD_SCATTER = 2,  /*   scatter */
+    PJ_STAGE_BUILD_PASS2 = 3,    /* pass two of the build side (empty for one-pass plans) */
+    PJ_STAGE_PROBE_HIST = 4,
+    PJ_STAGE_PROBE_SCAN = 5,
+    PJ_STAGE_PROBE_SCATTER = 6,
+    PJ_STAGE_PROBE_PASS2 = 7,
+    PJ_STAGE_JOIN_PLAN = 8,      /* work split: the reference's handle_skewed_data */
+    PJ_STAGE_JOIN = 9,
+    PJ_STAGE_TOTAL = 10,
+    PJ_NUM_STAGES = 11
 };
 
 /* pj_inner_join with a cudaEvent around every stage; SYNCHRONISES the
@@ -216,6 +230,19 @@ pj_status pj_inner_join_events(const pj_join_desc* desc, const pj_plan* plan, pj
  * call that used this workspace (PJ_OK, PJ_ERR_CAPACITY, PJ_ERR_OVERFLOW,
  * PJ_ERR_TIMEOUT or PJ_ERR_INTERNAL), then clears it. */
 pj_status pj_check(void* workspace, pj_stream stream);
+
+/* Diagnostics of the bounded device waits (no reference counterpart: the
+ * reference's only bounded loop is the build insert's attempt counter,
+ * hash_join_kernels.cuh:104-127).  Runs the build side's decoupled
+ * look-back scan in the workspace of (desc, plan) with the publish of tile
+ * `withhold_tile` withheld, so the tiles after it poll at most
+ * `spin_limit` times and give up.  pj_check then returns PJ_ERR_TIMEOUT;
+ * the context stays usable and the next join on the workspace starts
+ * clean.  Needs withhold_tile + 1 < the scan's tile count (4096 counters
+ * a tile); asynchronous. */
+pj_status pj_diag_scan_timeout(const pj_join_desc* desc, const pj_plan* plan, void* workspace,
+                               size_t workspace_bytes, int64_t withhold_tile, uint32_t spin_limit,
+                               pj_stream stream);
 
 /* Size of the library's built-in workspace on each device (64 MiB). */
 #define PJ_NOALLOC_SCRATCH_BYTES (64u << 20)

@@ -16,8 +16,8 @@ SPLIT_HASH, SPLIT_POSITION = 0, 1
 TABLE_BUCKET, TABLE_OPEN, TABLE_COMPACT, TABLE_EXACT = 0, 1, 2, 3
 NOALLOC_SCRATCH_BYTES = 64 << 20  # PJ_NOALLOC_SCRATCH_BYTES
 MAX_HEAVY = 256                   # PJ_MAX_HEAVY
-STAGES = ["build_hist", "build_scan", "build_scatter", "probe_hist", "probe_scan", "probe_scatter", "join_plan",
-          "join", "total"]
+STAGES = ["build_hist", "build_scan", "build_scatter", "build_pass2", "probe_hist", "probe_scan", "probe_scatter",
+          "probe_pass2", "join_plan", "join", "total"]
 
 
 class JoinDesc(ctypes.Structure):
@@ -78,6 +78,7 @@ SIGNATURES = {
     "pj_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "pj_version": (ctypes.c_char_p, []),
     "pj_plan_default": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan)]),
+    "pj_plan_radix": (ctypes.c_int, [ctypes.POINTER(JoinDesc), _I32, _I32, ctypes.c_float, ctypes.POINTER(Plan)]),
     "pj_workspace_size": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), ctypes.POINTER(_SZ)]),
     "pj_plan_exact": (ctypes.c_int, [ctypes.POINTER(JoinDesc), _P, _SZ, ctypes.POINTER(Plan), _P]),
     "pj_inner_join": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), ctypes.POINTER(Output), _P, _SZ, _P]),
@@ -87,6 +88,8 @@ SIGNATURES = {
                                             _SZ, _P, ctypes.POINTER(ctypes.c_void_p)]),
     "pj_join_count": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), _P, _P, _SZ, _P]),
     "pj_check": (ctypes.c_int, [_P, _P]),
+    "pj_diag_scan_timeout": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), _P, _SZ, _I64,
+                                            ctypes.c_uint32, _P]),
     "pj_inner_join_noalloc": (ctypes.c_int, [ctypes.POINTER(JoinDesc), ctypes.POINTER(Plan), ctypes.POINTER(Output), _P]),
     "pj_hash_keys": (ctypes.c_int, [_P, _I64, _I32, _P, _P]),
     "pj_hash_slots": (ctypes.c_int, [_P, _I64, _I32, _I32, _I32, _I32, _P, _P]),

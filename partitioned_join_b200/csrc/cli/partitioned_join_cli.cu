@@ -8,13 +8,17 @@
 //  * Tables are generated on the device by pj_generate_tables (same recipe
 //    as generate_input_tables.cuh; rand_max defaults to twice the default
 //    build size, 2^21, as main.cu:79 computes it before parsing).
-//  * -n/-N/-R/-f/-H describe the reference's partitioning; they are
-//    accepted and reported, but the plan comes from pj_plan_exact (exact
-//    histograms) and the library's one-pass partitioning.  The CSV columns
-//    keep their meaning: "part P1" is all partitioning (histograms, scans,
-//    scatters of both sides), "part P2" 0, "handle skew" the work split,
-//    "join" the build/probe kernel, "total" their sum.  With -H the
-//    histogram time is reported under "combined histo".
+//  * -n, -R -N and -f plan the join as the reference's flags do
+//    (pj_plan_radix: 2^log2(n) first-pass partitions by raw key bits, with -R
+//    a second pass into N partitions each, build pieces of at most
+//    ceil(f * |R| / partitions) rows).  The second pass splits by hash bits
+//    rather than the key's low bits.  Without -n the exact-histogram planner
+//    chooses (pj_plan_exact); the reference requires -n.  The CSV columns
+//    keep their meaning: "part P1" is the first pass of both sides
+//    (histograms, scans, scatters), "part P2" the second pass of both sides,
+//    "handle skew" the work split, "join" the build/probe kernel, "total"
+//    their sum.  With -H the first pass's histogram time is reported under
+//    "combined histo".
 //  * The check (without -S) does not re-run the join on the CPU: every
 //    output pair is verified on the device (both rows in range and their
 //    keys equal), and for unique build keys the pair count must equal the
@@ -110,10 +114,10 @@ void usage()
         {"B", "build_tbl_file [arg]", "Build table file path [default: ]"},
         {"P", "probe_tbl_file [arg]", "Probe table file path [default: ]"},
         {"v", "verbosity [arg]", "Verbosity level [default: 0]"},
-        {"f", "max_partition_size_factor [arg]", "Max partition size factor (reported) [default: 3.000000]"},
-        {"R", "radix_partition", "Two-pass radix partition (reported) [default: false]"},
-        {"n", "num_partitions_1 [arg]", "Number of partitions for pass 1 (reported) [default: -1]"},
-        {"N", "num_partitions_2 [arg]", "Number of partitions for pass 2 (reported) [default: -1]"},
+        {"f", "max_partition_size_factor [arg]", "Max partition size factor [default: 3.000000]"},
+        {"R", "radix_partition", "Two-pass radix partition [default: false]"},
+        {"n", "num_partitions_1 [arg]", "Number of partitions for pass 1 (none: exact-histogram plan) [default: -1]"},
+        {"N", "num_partitions_2 [arg]", "Number of partitions for pass 2 [default: -1]"},
         {"S", "skip_cpu_run [arg]", "Skip the check and give the output size [default: -1]"},
         {"V", "with_value", "Add value columns to input tables [default: false]"},
         {"C", "csv", "Output results in csv format [default: false]"},
@@ -204,7 +208,10 @@ int run(Options& o)
         return 1;
     }
     int num_bits_1 = 0, num_bits_2 = 0;
-    if (!o.radix_partition && is_power_of_two(o.num_partitions_1)) {
+    const bool plan_from_flags = o.num_partitions_1 != -1 || o.radix_partition;
+    if (!plan_from_flags) {
+        // no partition flags: the exact-histogram planner chooses
+    } else if (!o.radix_partition && is_power_of_two(o.num_partitions_1)) {
         num_bits_1 = static_cast<int>(std::log2(o.num_partitions_1));
     } else if (o.radix_partition && is_power_of_two(o.num_partitions_1) && is_power_of_two(o.num_partitions_2)) {
         num_bits_1 = static_cast<int>(std::log2(o.num_partitions_1));
@@ -275,12 +282,23 @@ int run(Options& o)
         d.payload_bytes = 4;
     }
     pj_plan plan;
-    CLI_PJ(pj_plan_default(&d, &plan));
+    if (plan_from_flags) {
+        const pj_status ps = pj_plan_radix(&d, o.num_partitions_1, o.radix_partition ? o.num_partitions_2 : 0,
+                                           o.max_partition_size_factor, &plan);
+        if (ps != PJ_OK) {
+            std::cerr << "Error: partition flags -n " << o.num_partitions_1 << (o.radix_partition ? " -N " : "")
+                      << (o.radix_partition ? std::to_string(o.num_partitions_2) : std::string()) << " -f "
+                      << o.max_partition_size_factor << ": " << pj_status_string(ps) << std::endl;
+            return 1;
+        }
+    } else {
+        CLI_PJ(pj_plan_default(&d, &plan));
+    }
     size_t ws_bytes = 0;
     CLI_PJ(pj_workspace_size(&d, &plan, &ws_bytes));
     void* ws = nullptr;
     CLI_CUDA(cudaMalloc(&ws, ws_bytes));
-    if (nb > 0 && np > 0) {
+    if (!plan_from_flags && nb > 0 && np > 0) {
         CLI_PJ(pj_plan_exact(&d, ws, ws_bytes, &plan, nullptr));
         size_t need = 0;
         CLI_PJ(pj_workspace_size(&d, &plan, &need));
@@ -346,7 +364,9 @@ int run(Options& o)
             std::cout << "    num bits P2          = " << num_bits_2 << std::endl;
         }
         std::cout << "    B200 plan            = " << (1 << plan.bits1) << " partitions ("
-                  << (plan.digit_mode == PJ_DIGIT_RAW ? "raw key bits" : "hash bits") << "), "
+                  << (plan.digit_mode == PJ_DIGIT_RAW ? "raw key bits" : "hash bits") << ")";
+        if (plan.passes == 2) std::cout << " x " << (1 << plan.bits2) << " (hash bits)";
+        std::cout << ", "
                   << (plan.table_mode == PJ_TABLE_BUCKET    ? "bucket"
                       : plan.table_mode == PJ_TABLE_COMPACT ? "compact"
                       : plan.table_mode == PJ_TABLE_EXACT   ? "exact"
@@ -376,7 +396,7 @@ int run(Options& o)
         combined_histo_elapsed_ms = hist_ms;
         partition_one_elapsed_ms -= hist_ms;
     }
-    const float partition_two_elapsed_ms = 0;
+    const float partition_two_elapsed_ms = ms[PJ_STAGE_BUILD_PASS2] + ms[PJ_STAGE_PROBE_PASS2];
     const float data_skew_handle_elapsed_ms = ms[PJ_STAGE_JOIN_PLAN];
     const float join_elapsed_ms = ms[PJ_STAGE_JOIN];
     const float total_elapsed_ms = ms[PJ_STAGE_TOTAL];
@@ -417,7 +437,7 @@ int run(Options& o)
                       << " ms" << std::endl;
         std::cout << "    partition P1 time    = " << std::setprecision(3) << partition_one_elapsed_ms << " ms"
                   << std::endl;
-        if (o.radix_partition)
+        if (plan.passes == 2)
             std::cout << "    partition P2 time    = " << std::setprecision(3) << partition_two_elapsed_ms << " ms"
                       << std::endl;
         std::cout << "    skewed data time     = " << std::setprecision(3) << data_skew_handle_elapsed_ms << " ms"

@@ -424,7 +424,8 @@ Layout make_layout(const pj_join_desc* d, const pj_plan* p)
     L.item_part = take(4 * static_cast<size_t>(L.max_items));
     // output fix-up: per join CTA records, segments, and room for the
     // reserved positions past the caller's capacity (one chunk per CTA)
-    L.max_ctas = sm_count() * join_ctas_per_sm(d->key_bytes, p);
+    // the fix-up plan kernel records one gap per join CTA in a 1024-thread block
+    L.max_ctas = std::min(sm_count() * join_ctas_per_sm(d->key_bytes, p), MAX_FIXUP_CTAS);
     L.over_cap = static_cast<int64_t>(L.max_ctas) * OUT_CHUNK;
     L.cta_q = take(8 * static_cast<size_t>(L.max_ctas));
     L.cta_last = take(8 * static_cast<size_t>(L.max_ctas));
@@ -621,11 +622,12 @@ pj_status launch_hist(const K* keys, int64_t n, int64_t chunk, int items, int hs
 
 template <typename TIn>
 pj_status launch_scan(const TIn* in, int64_t m, uint32_t round_to, int64_t* out, uint64_t* tiles,
-                      uint32_t* tile_counter, uint32_t* status, cudaStream_t st)
+                      uint32_t* tile_counter, uint32_t* status, cudaStream_t st,
+                      ScanWait wait = ScanWait{-1, SPIN_LIMIT})
 {
     const int64_t ntiles = std::max<int64_t>(1, (m + SCAN_TILE - 1) / SCAN_TILE);
     lookback_scan_kernel<TIn><<<static_cast<unsigned>(ntiles), SCAN_THREADS, 0, st>>>(in, m, round_to, out, tiles,
-                                                                                    tile_counter, status);
+                                                                                    tile_counter, status, wait);
     PJ_CUDA(cudaGetLastError());
     return PJ_OK;
 }
@@ -688,7 +690,7 @@ pj_status launch_join_t(const JoinArgs& a, cudaStream_t st)
     kern<<<grid, JN_THREADS, smem, st>>>(a);
     PJ_CUDA(cudaGetLastError());
     // fix-up: dense output and the true count
-    join_fixup_plan_kernel<<<1, 1024, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.base_count, a.capacity,
+    join_fixup_plan_kernel<<<1, MAX_FIXUP_CTAS, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.base_count, a.capacity,
                                                a.out_build != nullptr ? 1 : 0, a.seg, a.status);
     PJ_CUDA(cudaGetLastError());
     if (a.out_build != nullptr) {
@@ -856,6 +858,7 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
         PJ_CUDA(cudaGetLastError());
     }
     const bool two = p->passes == 2;
+    E.mark(PJ_STAGE_BUILD_PASS2, st);
     if (two && (s = partition_pass2<K>(p, L, 0, ws, reinterpret_cast<uint32_t*>(ws + L.b_tuples2), L.b_cap2, st)) !=
                    PJ_OK)
         return s;
@@ -863,6 +866,7 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
                                  reinterpret_cast<uint32_t*>(ws + L.p_tuples), L.p_cap, E, PJ_STAGE_PROBE_HIST,
                                  st, hc)) != PJ_OK)
         return s;
+    E.mark(PJ_STAGE_PROBE_PASS2, st);
     if (two && (s = partition_pass2<K>(p, L, 1, ws, reinterpret_cast<uint32_t*>(ws + L.p_tuples2), L.p_cap2, st)) !=
                    PJ_OK)
         return s;
@@ -1095,6 +1099,31 @@ pj_status pj_plan_default(const pj_join_desc* d, pj_plan* p)
     return PJ_OK;
 }
 
+pj_status pj_plan_radix(const pj_join_desc* d, int32_t partitions_1, int32_t partitions_2, float factor, pj_plan* p)
+{
+    if (!valid_desc(d) || !p) return PJ_ERR_INVALID;
+    auto pow2 = [](int32_t x) { return x > 0 && (x & (x - 1)) == 0; };
+    if (!pow2(partitions_1) || (partitions_2 != 0 && !pow2(partitions_2))) return PJ_ERR_INVALID;  // main.cu:239-251
+    if (!(factor > 0.0f)) return PJ_ERR_INVALID;
+    pj_status s = pj_plan_default(d, p);
+    if (s != PJ_OK) return s;
+    const int b1 = ilog2_floor(partitions_1), b2 = partitions_2 ? ilog2_floor(partitions_2) : 0;
+    p->passes = partitions_2 ? 2 : 1;
+    p->bits1 = b1;
+    p->bits2 = b2;
+    p->digit_mode = PJ_DIGIT_RAW;  // the first pass's digit is raw key bits, as the reference's
+    p->table_mode = PJ_TABLE_BUCKET;
+    p->split_mode = PJ_SPLIT_POSITION;  // handle_skewed_data cuts partitions into build chunks by position
+    p->wc_tuples = pick_wc(d->key_bytes, b1);
+    if (p->wc_tuples == 0) return PJ_ERR_INVALID;  // beyond one scatter pass's fan-out
+    // the build chunk ceil(factor * |R| / partitions) (partitioned_join.cuh:198-206), within one table
+    const double parts = static_cast<double>(partitions_1) * (partitions_2 ? partitions_2 : 1);
+    const double chunk = std::ceil(static_cast<double>(factor) * static_cast<double>(d->n_build) / parts);
+    const int max_cap = max_table_capacity(d->key_bytes, PJ_TABLE_BUCKET);
+    p->table_capacity = static_cast<int32_t>(std::min<double>(max_cap, std::max(64.0, chunk)));
+    return check_plan(d, p);
+}
+
 pj_status pj_workspace_size(const pj_join_desc* d, const pj_plan* plan, size_t* bytes)
 {
     if (!valid_desc(d) || !bytes) return PJ_ERR_INVALID;
@@ -1188,6 +1217,26 @@ pj_status pj_check(void* ws, pj_stream stream)
     if (st & ST_OVERFLOW) return PJ_ERR_OVERFLOW;
     if (st & ST_CAPACITY) return PJ_ERR_CAPACITY;
     return PJ_OK;
+}
+
+pj_status pj_diag_scan_timeout(const pj_join_desc* d, const pj_plan* plan, void* ws, size_t ws_bytes,
+                               int64_t withhold_tile, uint32_t spin_limit, pj_stream stream)
+{
+    pj_plan p;
+    Layout L;
+    pj_status s = prepare(d, plan, ws, ws_bytes, &p, &L);
+    if (s != PJ_OK) return s;
+    const int64_t m = static_cast<int64_t>(L.P1) * L.b_items;
+    const int64_t ntiles = (m + SCAN_TILE - 1) / SCAN_TILE;
+    if (withhold_tile < 0 || withhold_tile + 1 >= ntiles || spin_limit == 0) return PJ_ERR_INVALID;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    PJ_CUDA(cudaMemsetAsync(w, 0, L.ctrl_end, st));  // as a join starts: zero counts, tile states, status
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(w + L.counters);
+    return launch_scan<uint32_t>(reinterpret_cast<const uint32_t*>(w + L.b_counts), m, 1u,
+                                 reinterpret_cast<int64_t*>(w + L.b_off), reinterpret_cast<uint64_t*>(w + L.b_tiles),
+                                 ctr + CTR_BTILE, reinterpret_cast<uint32_t*>(w + L.status), st,
+                                 ScanWait{withhold_tile, spin_limit});
 }
 
 pj_status pj_hash_keys(const void* keys, int64_t n, int32_t key_bytes, uint32_t* out, pj_stream stream)

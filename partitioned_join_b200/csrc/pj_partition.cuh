@@ -209,12 +209,21 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p)
     return v;
 }
 
+// The look-back wait of a scan: how many polls a tile makes before it gives
+// up (ST_TIMEOUT), and a tile that never publishes (-1: none).  Joins use
+// {-1, SPIN_LIMIT}; pj_diag_scan_timeout withholds a tile to show that a
+// wait which never ends returns an error instead of hanging.
+struct ScanWait {
+    int64_t withhold_tile;
+    uint32_t spin_limit;
+};
+
 template <typename TIn>
 __global__ void __launch_bounds__(SCAN_THREADS) lookback_scan_kernel(const TIn* __restrict__ in, int64_t m,
                                                                      uint32_t round_to, int64_t* __restrict__ out,
                                                                      uint64_t* __restrict__ tile_state,
                                                                      uint32_t* __restrict__ tile_counter,
-                                                                     uint32_t* __restrict__ status)
+                                                                     uint32_t* __restrict__ status, ScanWait wait)
 {
     __shared__ uint32_t s_tile;
     __shared__ int64_t s_warp[SCAN_THREADS / 32];
@@ -259,7 +268,9 @@ __global__ void __launch_bounds__(SCAN_THREADS) lookback_scan_kernel(const TIn* 
 
     if (threadIdx.x == 0) {
         int64_t excl = 0;
-        if (tile == 0) {
+        if (tile == wait.withhold_tile) {
+            // publishes nothing: its successors' waits run out
+        } else if (tile == 0) {
             st_release_u64(&tile_state[0], TS_PREFIX | static_cast<uint64_t>(block_total));
         } else {
             st_release_u64(&tile_state[tile], TS_AGG | static_cast<uint64_t>(block_total));
@@ -269,7 +280,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) lookback_scan_kernel(const TIn* 
                 const uint64_t s = ld_acquire_u64(&tile_state[i]);
                 const uint64_t flag = s & ~TS_VALUE;
                 if (flag == 0) {
-                    if (++spins > SPIN_LIMIT) {
+                    if (++spins > wait.spin_limit) {
                         raise_status(status, ST_TIMEOUT);
                         break;
                     }

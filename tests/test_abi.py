@@ -76,3 +76,25 @@ def test_invalid_arguments_rejected(L):
     out.count = 16
     assert L.pj_inner_join(ctypes.byref(d), None, ctypes.byref(out), None, 0, None) == _lib.ERR_WORKSPACE
     assert L.pj_hash_keys(None, 10, 4, None, None) == _lib.ERR_INVALID
+
+
+def test_plan_radix_follows_the_reference_flags(L):
+    """pj_plan_radix: -n P1 [-R -N P2] -f factor (main.cu:239-251,867)."""
+    import math
+
+    from partitioned_join_b200 import _lib, api
+    d = api.desc_for_sizes(1 << 24, 1 << 24, 4)
+    p = _lib.Plan()
+    assert L.pj_plan_radix(ctypes.byref(d), 256, 512, ctypes.c_float(3.0), ctypes.byref(p)) == _lib.OK
+    assert (p.passes, p.bits1, p.bits2) == (2, 8, 9)
+    assert p.digit_mode == _lib.DIGIT_RAW and p.split_mode == _lib.SPLIT_POSITION
+    assert p.table_capacity == max(64, math.ceil(3.0 * (1 << 24) / (256 * 512)))
+    assert L.pj_plan_radix(ctypes.byref(d), 1024, 0, ctypes.c_float(1.0), ctypes.byref(p)) == _lib.OK
+    assert (p.passes, p.bits1, p.bits2) == (1, 10, 0)
+    # a build chunk larger than one table is capped at the table
+    assert p.table_capacity == api.plan_default(1 << 24, 1 << 24, 4).table_capacity or p.table_capacity < (1 << 24) // 1024 + 1
+    n = ctypes.c_size_t()
+    assert L.pj_workspace_size(ctypes.byref(d), ctypes.byref(p), ctypes.byref(n)) == _lib.OK
+    for bad in ((100, 0, 3.0), (256, 100, 3.0), (256, 0, 0.0), (0, 0, 3.0)):
+        assert L.pj_plan_radix(ctypes.byref(d), bad[0], bad[1], ctypes.c_float(bad[2]), ctypes.byref(p)) == \
+            _lib.ERR_INVALID, bad

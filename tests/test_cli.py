@@ -78,3 +78,23 @@ def test_cli_reads_key_files(tmp_path):
     f = _csv_fields(r.stdout)
     assert int(f[11]) == oracle.inner_join(b, p, True)[0].shape[0]
     assert int(f[18]) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags,parts,two", [(["-n", 64], "64 partitions (raw key bits), ", False),
+                                             (["-n", 1024], "1024 partitions (raw key bits), ", False),
+                                             (["-R", "-n", 256, "-N", 512], "256 partitions (raw key bits) x 512", True),
+                                             (["-R", "-n", 32, "-N", 16, "-f", 1.5], "32 partitions (raw key bits) x 16",
+                                              True)])
+def test_cli_plans_from_the_reference_partition_flags(flags, parts, two):
+    b = 1 << 22
+    args = ["-b", b, "-p", b, "-r", 2 * b, "-u", "-s", 0.9, *flags]
+    r = run_cli(*args)
+    assert r.returncode == 0, r.stderr
+    assert f"B200 plan            = {parts}" in r.stdout
+    assert "number of errors     = 0" in r.stdout
+    assert ("partition P2 time" in r.stdout) == two
+    f = _csv_fields(run_cli(*args, "-C").stdout)
+    assert int(f[18]) == 0 and abs(int(f[11]) / b - 0.9) < 0.01
+    assert (float(f[14]) > 0) == two  # part P2 [ms]: the second pass's own time
+    assert float(f[13]) > 0
