@@ -307,13 +307,18 @@ pj_status pj_partition(const void* keys, int64_t n, int32_t key_bytes, const pj_
  * Joins whose build side fits one shared-memory table skip partitioning: one
  * persistent kernel drains a (join, probe chunk) work queue over all of
  * them, writing each join's pairs densely to its own output.  Larger joins
- * take the partitioned path, one after another in a reused workspace
- * region.  All joins of a batch have the same key width. */
+ * (up to 2^10 partitions each) are partitioned together -- one histogram,
+ * one scan and one scatter launch over both key columns of all of them --
+ * and joined by one persistent launch that drains a (join, partition, probe
+ * chunk) queue, each match written at an exact position of its join's
+ * output.  Wider joins run the partitioned path one after another.  All
+ * joins of a batch have the same key width. */
 typedef struct pj_batch_config {
     int32_t direct_threads;    /* threads per CTA of the direct kernel: 256, 512 or 1024 */
     int32_t direct_chunk;      /* probe rows per direct work item (>= 1024) */
     int32_t direct_max_build;  /* joins with at most this many build rows go direct (<= 40960) */
     int32_t large_bits_delta;  /* added to the default radix bits of the partitioned joins */
+    int32_t large_batched;     /* 1: partitioned joins run together (above); 0: one after another */
 } pj_batch_config;
 
 /* Defaults for a key width. */
@@ -341,7 +346,8 @@ pj_status pj_batch_check(void* workspace, pj_stream stream);
 
 /* Autotuner: times candidate configurations on this batch (where the
  * direct path ends, the direct kernel's block size and chunk, the radix
- * width of the partitioned joins) and returns the fastest in *best (and its
+ * width of the partitioned joins, whether they run together) and returns the
+ * fastest in *best (and its
  * time, optional).  SYNCHRONISES; runs the batch many times.  The workspace
  * must hold pj_batch_workspace_size for direct_max_build = 0. */
 pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, int32_t n, void* workspace,

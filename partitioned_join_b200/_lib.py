@@ -59,7 +59,8 @@ class Plan(ctypes.Structure):
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("direct_threads", ctypes.c_int32), ("direct_chunk", ctypes.c_int32),
-                ("direct_max_build", ctypes.c_int32), ("large_bits_delta", ctypes.c_int32)]
+                ("direct_max_build", ctypes.c_int32), ("large_bits_delta", ctypes.c_int32),
+                ("large_batched", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -288,13 +288,15 @@ class BatchJoiner:
         worst = _lib.BatchConfig.from_buffer_copy(self.config)
         worst.direct_max_build = 0
         self.ws_bytes = max(self._ws_size(self.config), self._ws_size(worst))
-        for d in (-1, 1):
-            c = _lib.BatchConfig.from_buffer_copy(worst)
-            c.large_bits_delta = d
-            try:
-                self.ws_bytes = max(self.ws_bytes, self._ws_size(c))
-            except PJError:
-                pass
+        for together in (1, 0):
+            for d in (-1, 0, 1):
+                c = _lib.BatchConfig.from_buffer_copy(worst)
+                c.large_bits_delta = d
+                c.large_batched = together
+                try:
+                    self.ws_bytes = max(self.ws_bytes, self._ws_size(c))
+                except PJError:
+                    pass
         self.ws = alloc_workspace(self.ws_bytes, dev)
         self.prepare()
 

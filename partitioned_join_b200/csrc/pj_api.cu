@@ -13,6 +13,7 @@
 
 #include "../../include/pj.h"
 #include "pj_device.cuh"
+#include "pj_internal.h"
 #include "pj_join.cuh"
 #include "pj_partition.cuh"
 
@@ -887,7 +888,7 @@ pj_status run_join(const pj_join_desc* d, const pj_plan* p, const Layout& L, uin
         reinterpret_cast<int64_t*>(ws + jb_off), reinterpret_cast<int64_t*>(ws + jp_off), jb_items, jp_items,
         L.P, reinterpret_cast<int32_t*>(ws + L.b_tot), reinterpret_cast<int32_t*>(ws + L.p_tot),
         hash_split ? cap_tuples : position_chunk, p->probe_chunk, hash_split ? 1 : 0, MAX_SPLIT_LOG2,
-        reinterpret_cast<int32_t*>(ws + L.split), reinterpret_cast<int64_t*>(ws + L.items), status);
+        reinterpret_cast<int32_t*>(ws + L.split), reinterpret_cast<int64_t*>(ws + L.items), status, nullptr);
     PJ_CUDA(cudaGetLastError());
     if ((s = launch_scan<int64_t>(reinterpret_cast<int64_t*>(ws + L.items), L.P, 1u,
                                   reinterpret_cast<int64_t*>(ws + L.item_off), reinterpret_cast<uint64_t*>(ws + L.i_tiles),
@@ -1558,3 +1559,258 @@ pj_status pj_plan_learned(const pj_join_desc* d, const float* params, void* ws, 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// The partitioned joins of a batch, run together (pj_internal.h).
+namespace pj_internal {
+
+namespace {
+
+constexpr int64_t SEG_CHUNK = 1 << 16;  // rows of one scatter item of a batch segment
+
+template <typename K>
+pj_status large_batch_run_t(const LargeBatch& lb, void* ws, uint32_t* status, cudaStream_t st)
+{
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(w + lb.o_counters);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(w + lb.o_counts);
+    int32_t* totals = reinterpret_cast<int32_t*>(w + lb.o_totals);
+    int64_t* off = reinterpret_cast<int64_t*>(w + lb.o_off);
+    uint32_t* tuples = reinterpret_cast<uint32_t*>(w + lb.o_tuples);
+    const SegItem* items = reinterpret_cast<const SegItem*>(w + lb.o_items);
+    const int n_items = static_cast<int>(lb.seg.size());
+    PJ_CUDA(cudaMemsetAsync(w + lb.o_ctrl, 0, lb.ctrl_bytes, st));
+    const int n_jobs = static_cast<int>(lb.joins.size());
+    zero_job_counts_kernel<<<(n_jobs + 255) / 256, 256, 0, st>>>(reinterpret_cast<const JobOut*>(w + lb.o_outs), n_jobs);
+    PJ_CUDA(cudaGetLastError());
+    // histogram, scan, scatter over every segment of every join
+    const size_t hsmem = 4 * static_cast<size_t>((lb.Pmax + 3) & ~3);
+    PJ_CUDA(set_smem(hist_seg_kernel<K>, hsmem));
+    hist_seg_kernel<K><<<static_cast<unsigned>(n_items) * 2, HIST_THREADS, hsmem, st>>>(items, 2, counts, totals);
+    PJ_CUDA(cudaGetLastError());
+    pj_status s;
+    if ((s = launch_scan<uint32_t>(counts, lb.n_counts, static_cast<uint32_t>(lb.W), off,
+                                   reinterpret_cast<uint64_t*>(w + lb.o_tiles), ctr + CTR_BTILE, status, st)) != PJ_OK)
+        return s;
+    constexpr int VT = sizeof(K) == 4 ? 4 : 2;
+    const size_t ssmem = scatter_smem(sizeof(K), lb.wc_cap, lb.Pmax);
+    const uint32_t out_cap = static_cast<uint32_t>(std::min<int64_t>(lb.tuples, UINT32_MAX));
+    const int sgrid = std::min(n_items, sm_count());
+    switch (lb.W) {
+    case 4: {
+        auto* k = scatter_seg_kernel<K, SC_THREADS, VT, 4>;
+        PJ_CUDA(set_smem(k, ssmem));
+        k<<<sgrid, SC_THREADS, ssmem, st>>>(items, n_items, lb.Pmax, lb.wc_cap, off, tuples, out_cap, status);
+        break;
+    }
+    case 2: {
+        auto* k = scatter_seg_kernel<K, SC_THREADS, VT, 2>;
+        PJ_CUDA(set_smem(k, ssmem));
+        k<<<sgrid, SC_THREADS, ssmem, st>>>(items, n_items, lb.Pmax, lb.wc_cap, off, tuples, out_cap, status);
+        break;
+    }
+    default: return PJ_ERR_INVALID;
+    }
+    PJ_CUDA(cudaGetLastError());
+    // work split over all partitions, then one join launch
+    const PartRef* parts = reinterpret_cast<const PartRef*>(w + lb.o_parts);
+    const int cap_tuples = lb.table_cap;
+    const bool hash_split = lb.unique;
+    const int position_chunk = std::max(16, cap_tuples / 16 * 16);
+    join_items_kernel<<<(lb.G + 255) / 256, 256, 0, st>>>(
+        off, off, 1, 1, lb.G, totals, totals + lb.G, hash_split ? cap_tuples : position_chunk, lb.probe_chunk,
+        hash_split ? 1 : 0, MAX_SPLIT_LOG2, reinterpret_cast<int32_t*>(w + lb.o_split),
+        reinterpret_cast<int64_t*>(w + lb.o_jitems), status, parts);
+    PJ_CUDA(cudaGetLastError());
+    if ((s = launch_scan<int64_t>(reinterpret_cast<int64_t*>(w + lb.o_jitems), lb.G, 1u,
+                                  reinterpret_cast<int64_t*>(w + lb.o_item_off),
+                                  reinterpret_cast<uint64_t*>(w + lb.o_itiles), ctr + CTR_ITILE, status, st)) != PJ_OK)
+        return s;
+    items_expand_kernel<<<lb.G, 256, 0, st>>>(reinterpret_cast<int64_t*>(w + lb.o_item_off), lb.G,
+                                              reinterpret_cast<int32_t*>(w + lb.o_item_part), lb.max_items, status);
+    PJ_CUDA(cudaGetLastError());
+    JoinArgs a{};
+    a.build_tuples = a.probe_tuples = tuples;
+    a.build_off = a.probe_off = off;
+    a.b_items = a.p_items = 1;
+    a.P = lb.G;
+    a.split = reinterpret_cast<const int32_t*>(w + lb.o_split);
+    a.item_off = reinterpret_cast<const int64_t*>(w + lb.o_item_off);
+    a.item_part = reinterpret_cast<const int32_t*>(w + lb.o_item_part);
+    a.max_items = lb.max_items;
+    a.queue = ctr + CTR_QUEUE;
+    a.cap = lb.table_cap;
+    a.nb_log2 = lb.nb_log2;
+    a.probe_chunk = lb.probe_chunk;
+    a.position_chunk = position_chunk;
+    a.status = status;
+    a.parts = parts;
+    a.outs = reinterpret_cast<const JobOut*>(w + lb.o_outs);
+    auto launch = [&](auto* kern) -> pj_status {
+        const size_t smem = JoinSmem<K, TABLE_BUCKET>::bytes(a.cap, a.nb_log2, JN_THREADS);
+        PJ_CUDA(set_smem(kern, smem));
+        int per_sm = 0;
+        PJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, JN_THREADS, smem));
+        per_sm = std::min(std::max(per_sm, 1), MAX_JOIN_CTAS_PER_SM);
+        kern<<<sm_count() * per_sm, JN_THREADS, smem, st>>>(a);
+        PJ_CUDA(cudaGetLastError());
+        return PJ_OK;
+    };
+    if (lb.unique) return launch(join_kernel<K, TABLE_BUCKET, true, true, false, JN_THREADS, true>);
+    return launch(join_kernel<K, TABLE_BUCKET, false, false, false, JN_THREADS, true>);
+}
+
+}  // namespace
+
+pj_status large_batch_layout(const pj_join_desc* descs, const std::vector<int>& joins, int bits_delta, LargeBatch* out)
+{
+    LargeBatch lb;
+    if (joins.empty()) {
+        *out = lb;
+        return PJ_OK;
+    }
+    lb.key_bytes = descs[joins[0]].key_bytes;
+    lb.table_cap = max_table_capacity(lb.key_bytes, PJ_TABLE_BUCKET);
+    lb.nb_log2 = bucket_nb_log2(lb.table_cap);
+    int64_t probe_total = 0;
+    struct J { int idx, bits; };
+    std::vector<J> take;
+    for (int i : joins) {
+        const pj_join_desc& d = descs[i];
+        if (!valid_desc(&d) || d.key_bytes != lb.key_bytes) return PJ_ERR_INVALID;
+        if (d.n_build == 0 || d.n_probe == 0) continue;  // nothing to join: the count stays 0
+        const int bits = std::max(0, bits_for_table(d.n_build, lb.table_cap) + bits_delta);
+        if (bits > LARGE_BATCH_MAX_BITS) continue;  // (scalar key loads: no alignment needed)
+        take.push_back({i, bits});
+        lb.unique = lb.unique && d.unique_build_keys != 0;
+        probe_total += d.n_probe;
+    }
+    for (const J& j : take) lb.Pmax = std::max(lb.Pmax, 1 << j.bits);
+    lb.W = pick_wc(lb.key_bytes, ilog2_floor(lb.Pmax));
+    if (lb.W == 0) return PJ_ERR_INVALID;
+    lb.wc_cap = wc_cap(lb.key_bytes, lb.W, lb.Pmax, SC_THREADS * (lb.key_bytes == 4 ? 4 : 2), 0);
+    // probe chunks: about 8 work items per SM over the whole batch
+    {
+        const int64_t per = (probe_total + static_cast<int64_t>(sm_count()) * 8 - 1) / (static_cast<int64_t>(sm_count()) * 8);
+        lb.probe_chunk = static_cast<int32_t>(std::min<int64_t>(std::max<int64_t>(1 << 14, (per + 15) / 16 * 16), 1 << 30));
+    }
+    int64_t cnt = 0, tup = 0, max_items = 0;
+    int g = 0;
+    for (const J& j : take) {
+        const pj_join_desc& d = descs[j.idx];
+        const int P = 1 << j.bits;
+        DigitFn f{PJ_DIGIT_HASH, j.bits ? 32 - j.bits : 0, static_cast<uint32_t>(P - 1)};
+        int64_t base[2];
+        int32_t nit[2];
+        for (int side = 0; side < 2; ++side) {
+            const int64_t n = side == 0 ? d.n_build : d.n_probe;
+            const int items = static_cast<int>(std::max<int64_t>(1, (n + SEG_CHUNK - 1) / SEG_CHUNK));
+            const int64_t chunk = chunk_for(n, items);
+            base[side] = cnt;
+            nit[side] = items;
+            for (int i = 0; i < items; ++i) {
+                SegItem it{};
+                it.keys = side == 0 ? d.build_keys : d.probe_keys;
+                it.lo = std::min<int64_t>(n, static_cast<int64_t>(i) * chunk);
+                it.hi = std::min<int64_t>(n, it.lo + chunk);
+                it.cnt_base = cnt;
+                it.seg_items = items;
+                it.item = i;
+                it.tot_base = 0;  // set below, once G is known
+                it.P = P;
+                it.f = f;
+                lb.seg.push_back(it);
+            }
+            cnt += static_cast<int64_t>(P) * items;
+            tup += part_capacity(n, P, items, lb.W);
+        }
+        for (int p = 0; p < P; ++p) {
+            PartRef r{};
+            r.b_at = base[0] + static_cast<int64_t>(p) * nit[0];
+            r.p_at = base[1] + static_cast<int64_t>(p) * nit[1];
+            r.b_items = nit[0];
+            r.p_items = nit[1];
+            r.job = static_cast<int32_t>(lb.joins.size());
+            r.digit_bits = j.bits;
+            lb.parts.push_back(r);
+        }
+        // work items: each partition's hash pieces times its probe chunks
+        const int64_t max_pieces = static_cast<int64_t>(P) << MAX_SPLIT_LOG2;
+        max_items += std::min<int64_t>(max_pieces * (P + part_capacity(d.n_probe, P, nit[1], lb.W) / lb.probe_chunk + 1),
+                                       static_cast<int64_t>(P) * 4096 + max_pieces + P +
+                                           part_capacity(d.n_probe, P, nit[1], lb.W) / lb.probe_chunk + 1);
+        lb.joins.push_back(j.idx);
+        g += P;
+    }
+    lb.G = g;
+    // tot_base: build totals at [0, G), probe totals at [G, 2G)
+    {
+        size_t at = 0;
+        int gb = 0;
+        for (const J& j : take) {
+            const pj_join_desc& d = descs[j.idx];
+            const int P = 1 << j.bits;
+            for (int side = 0; side < 2; ++side) {
+                const int64_t n = side == 0 ? d.n_build : d.n_probe;
+                const int items = static_cast<int>(std::max<int64_t>(1, (n + SEG_CHUNK - 1) / SEG_CHUNK));
+                for (int i = 0; i < items; ++i) lb.seg[at++].tot_base = side == 0 ? gb : lb.G + gb;
+            }
+            gb += P;
+        }
+    }
+    lb.n_counts = cnt;
+    lb.tuples = tup + 64;
+    if (lb.tuples >= static_cast<int64_t>(UINT32_MAX)) return PJ_ERR_INVALID;
+    lb.max_items = std::min<int64_t>(max_items, int64_t(1) << 30);
+    lb.tiles_n = (lb.n_counts + SCAN_TILE - 1) / SCAN_TILE + 1;
+    lb.itiles_n = (lb.G + SCAN_TILE - 1) / SCAN_TILE + 1;
+    size_t o = 0;
+    auto take_b = [&](size_t bytes) { const size_t at = o; o = align_up(o + bytes, 256); return at; };
+    lb.o_ctrl = take_b(0);
+    lb.o_counters = take_b(4 * 8);
+    lb.o_counts = take_b(4 * static_cast<size_t>(lb.n_counts));
+    lb.o_totals = take_b(4 * 2 * static_cast<size_t>(lb.G));
+    lb.o_tiles = take_b(8 * static_cast<size_t>(lb.tiles_n));
+    lb.o_itiles = take_b(8 * static_cast<size_t>(lb.itiles_n));
+    lb.ctrl_bytes = o - lb.o_ctrl;
+    lb.o_items = take_b(sizeof(SegItem) * lb.seg.size());
+    lb.o_parts = take_b(sizeof(PartRef) * lb.parts.size());
+    lb.o_outs = take_b(sizeof(JobOut) * lb.joins.size());
+    lb.o_off = take_b(8 * static_cast<size_t>(lb.n_counts + 1));
+    lb.o_split = take_b(4 * static_cast<size_t>(lb.G));
+    lb.o_jitems = take_b(8 * static_cast<size_t>(lb.G));
+    lb.o_item_off = take_b(8 * static_cast<size_t>(lb.G + 1));
+    lb.o_item_part = take_b(4 * static_cast<size_t>(lb.max_items));
+    lb.o_tuples = take_b(4 * static_cast<size_t>(tuple_words(lb.key_bytes)) * lb.tuples + 64);
+    lb.total = o;
+    *out = std::move(lb);
+    return PJ_OK;
+}
+
+pj_status large_batch_upload(const LargeBatch& lb, const pj_output* outs, void* ws, cudaStream_t st)
+{
+    if (lb.joins.empty()) return PJ_OK;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    std::vector<JobOut> jo(lb.joins.size());
+    for (size_t i = 0; i < lb.joins.size(); ++i) {
+        const pj_output& o = outs[lb.joins[i]];
+        jo[i] = JobOut{o.capacity > 0 ? o.build_row : nullptr, o.probe_row, o.capacity,
+                       reinterpret_cast<unsigned long long*>(o.count)};
+        if (o.capacity == 0) jo[i].out_build = nullptr;
+    }
+    PJ_CUDA(cudaMemcpyAsync(w + lb.o_items, lb.seg.data(), sizeof(SegItem) * lb.seg.size(), cudaMemcpyHostToDevice, st));
+    PJ_CUDA(cudaMemcpyAsync(w + lb.o_parts, lb.parts.data(), sizeof(PartRef) * lb.parts.size(), cudaMemcpyHostToDevice,
+                            st));
+    PJ_CUDA(cudaMemcpyAsync(w + lb.o_outs, jo.data(), sizeof(JobOut) * jo.size(), cudaMemcpyHostToDevice, st));
+    PJ_CUDA(cudaStreamSynchronize(st));
+    return PJ_OK;
+}
+
+pj_status large_batch_run(const LargeBatch& lb, void* ws, uint32_t* status, cudaStream_t st)
+{
+    if (lb.joins.empty()) return PJ_OK;
+    return lb.key_bytes == 4 ? large_batch_run_t<int32_t>(lb, ws, status, st)
+                             : large_batch_run_t<int64_t>(lb, ws, status, st);
+}
+
+}  // namespace pj_internal

@@ -12,9 +12,14 @@
 //     and stays in L2).  Matches go straight to the join's output at exact
 //     positions (one atomic on the join's counter per warp step), so every
 //     output is dense without a fix-up.
-//   * larger joins run the partitioned path (pj_inner_join) one after the
-//     other in one reused workspace region, their device status folded into
-//     the batch's.
+//   * larger joins (up to 2^10 partitions each) take the partitioned path
+//     together (pj_internal::large_batch_*): one histogram, one scan and one
+//     scatter launch over both key columns of all of them, then one work
+//     split and one persistent join launch over all their partitions, each
+//     match written at an exact position of its join's output.
+//   * wider joins (or with large_batched = 0, every larger join) run the
+//     partitioned path (pj_inner_join) one after the other in one reused
+//     workspace region, their device status folded into the batch's.
 // pj_batch_prepare writes the work table once (synchronous); pj_join_batch
 // then only enqueues kernels, so it can be captured in a CUDA graph and
 // replayed.  pj_batch_autotune measures candidate configurations on the
@@ -28,6 +33,7 @@
 
 #include "../../include/pj.h"
 #include "pj_device.cuh"
+#include "pj_internal.h"
 
 using namespace pj;
 
@@ -258,7 +264,9 @@ pj_plan large_plan(const pj_join_desc& d, const pj_batch_config& cfg, bool* ok)
 }
 
 struct BatchLayout {
-    size_t ctrl = 0, jobs = 0, large = 0, large_bytes = 0, total = 0;
+    size_t ctrl = 0, jobs = 0, large = 0, large_bytes = 0, batched = 0, total = 0;
+    pj_internal::LargeBatch lb;  // the larger joins run together
+    std::vector<int> sequential; // the larger joins run one after another
 };
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -269,9 +277,15 @@ pj_status layout_for(const pj_join_desc* descs, int32_t n, const pj_batch_config
     b.ctrl = 0;
     b.jobs = 256;
     b.large = align256(b.jobs + sizeof(BatchJob) * static_cast<size_t>(std::max(n, 1)));
-    for (int i = 0; i < n; ++i) {
+    const Split sp = split_batch(descs, n, cfg);
+    if (cfg.large_batched) {
+        pj_status s = pj_internal::large_batch_layout(descs, sp.large, cfg.large_bits_delta, &b.lb);
+        if (s != PJ_OK) return s;
+    }
+    for (int i : sp.large)
+        if (std::find(b.lb.joins.begin(), b.lb.joins.end(), i) == b.lb.joins.end()) b.sequential.push_back(i);
+    for (int i : b.sequential) {
         const pj_join_desc& d = descs[i];
-        if (d.n_build <= cfg.direct_max_build && d.n_build > 0 && d.n_probe > 0) continue;
         bool ok = false;
         pj_plan p = large_plan(d, cfg, &ok);
         if (!ok) return PJ_ERR_INVALID;
@@ -280,8 +294,9 @@ pj_status layout_for(const pj_join_desc* descs, int32_t n, const pj_batch_config
         if (s != PJ_OK) return s;
         b.large_bytes = std::max(b.large_bytes, w);
     }
-    b.total = b.large + align256(b.large_bytes);
-    *L = b;
+    b.batched = b.large + align256(b.large_bytes);
+    b.total = b.batched + align256(b.lb.total);
+    *L = std::move(b);
     return PJ_OK;
 }
 
@@ -292,6 +307,7 @@ pj_status check_batch(const pj_join_desc* descs, const pj_output* outs, int32_t 
     if (cfg->direct_chunk < 1024 || cfg->direct_max_build < 0 || cfg->direct_max_build > DIRECT_MAX_BUILD)
         return PJ_ERR_INVALID;
     if (cfg->large_bits_delta < -4 || cfg->large_bits_delta > 4) return PJ_ERR_INVALID;
+    if (cfg->large_batched != 0 && cfg->large_batched != 1) return PJ_ERR_INVALID;
     for (int i = 0; i < n; ++i) {
         if (descs[i].key_bytes != descs[0].key_bytes) return PJ_ERR_INVALID;  // one key width per batch
         if (outs) {
@@ -362,8 +378,9 @@ pj_status run_batch(const pj_join_desc* descs, const pj_output* outs, int32_t n,
         if (s != PJ_OK) return s;
     }
     if (parts & 2) {
+        if ((s = pj_internal::large_batch_run(L.lb, w + L.batched, status, st)) != PJ_OK) return s;
         void* lws = w + L.large;
-        for (int i : sp.large) {
+        for (int i : L.sequential) {
             bool ok = false;
             const pj_plan p = large_plan(descs[i], cfg, &ok);
             pj_output o = outs[i];
@@ -387,6 +404,7 @@ pj_status pj_batch_config_default(int32_t key_bytes, pj_batch_config* cfg)
     cfg->direct_chunk = 1 << 16;
     cfg->direct_max_build = key_bytes == 4 ? 20480 : 16384;
     cfg->large_bits_delta = 0;
+    cfg->large_batched = 1;
     return PJ_OK;
 }
 
@@ -441,6 +459,7 @@ pj_status pj_batch_prepare(const pj_join_desc* descs, const pj_output* outs, int
     if (!jobs.empty() &&
         cudaMemcpyAsync(w + L.jobs, jobs.data(), sizeof(BatchJob) * jobs.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return PJ_ERR_CUDA;
+    if ((s = pj_internal::large_batch_upload(L.lb, outs, w + L.batched, st)) != PJ_OK) return s;
     return cudaStreamSynchronize(st) == cudaSuccess ? PJ_OK : PJ_ERR_CUDA;
 }
 
@@ -533,19 +552,24 @@ pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, in
                 }
         }
     }
-    // 3. radix width of the partitioned joins (large part timed)
+    // 3. radix width of the partitioned joins, and whether they run
+    //    together or one after another (large part timed)
     if (s == PJ_OK) {
         float lbest = 0;
         if (time_cfg(cur, 2, &lbest) == PJ_OK) {
-            for (int dlt : {-1, 1}) {
-                pj_batch_config c = cur;
-                c.large_bits_delta = dlt;
-                float t = 0;
-                if (time_cfg(c, 2, &t) == PJ_OK && t < lbest) {
-                    lbest = t;
-                    cur.large_bits_delta = dlt;
+            for (int together : {1, 0})
+                for (int dlt : {-1, 0, 1}) {
+                    if (together == cur.large_batched && dlt == cur.large_bits_delta) continue;
+                    pj_batch_config c = cur;
+                    c.large_bits_delta = dlt;
+                    c.large_batched = together;
+                    float t = 0;
+                    if (time_cfg(c, 2, &t) == PJ_OK && t < lbest) {
+                        lbest = t;
+                        cur.large_bits_delta = dlt;
+                        cur.large_batched = together;
+                    }
                 }
-            }
         }
     }
     if (s == PJ_OK) {

@@ -46,12 +46,18 @@
 #include <cuda_runtime.h>
 
 #include "pj_device.cuh"
+#include "pj_types.cuh"
 
 namespace pj {
 
 constexpr uint32_t EMPTY_ROW = 0xffffffffu;
 enum : int { TABLE_BUCKET = 0, TABLE_OPEN = 1, TABLE_COMPACT = 2, TABLE_EXACT = 3 };
 constexpr int64_t COMPACT_RANGE = 65536;  // build range a COMPACT entry's index can address
+
+__global__ void zero_job_counts_kernel(const JobOut* __restrict__ outs, int32_t n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) *outs[i].count = 0;
+}
 
 struct JoinArgs {
     const uint32_t* build_tuples;
@@ -85,20 +91,31 @@ struct JoinArgs {
     int64_t* seg;               // fix-up segments
     int32_t max_ctas;           // join CTAs the fix-up records have room for
     const unsigned long long* base_count;  // entries written before the join (heavy keys), or nullptr
+    const PartRef* parts;       // batches: per partition (else nullptr)
+    const JobOut* outs;         // batches: per join
 };
 
 // Items per partition (S_p x K_p) and the split of partition p.
+// Batches pass `parts` (the partition's segments); single joins nullptr.
 __global__ void join_items_kernel(const int64_t* __restrict__ build_off, const int64_t* __restrict__ probe_off,
                                   int32_t b_items, int32_t p_items, int32_t P,
                                   const int32_t* __restrict__ build_tot, const int32_t* __restrict__ probe_tot,
                                   int32_t cap_per_table, int32_t probe_chunk, int32_t hash_split,
                                   int32_t max_split_log2, int32_t* __restrict__ split_out,
-                                  int64_t* __restrict__ items_out, uint32_t* __restrict__ status)
+                                  int64_t* __restrict__ items_out, uint32_t* __restrict__ status,
+                                  const PartRef* __restrict__ parts)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
+    int64_t b_at = static_cast<int64_t>(p) * b_items, p_at = static_cast<int64_t>(p) * p_items;
+    if (parts) {
+        b_at = parts[p].b_at;
+        p_at = parts[p].p_at;
+        b_items = parts[p].b_items;
+        p_items = parts[p].p_items;
+    }
     const int64_t bc = build_tot[p], pc = probe_tot[p];
-    const int64_t prange = probe_off[static_cast<int64_t>(p + 1) * p_items] - probe_off[static_cast<int64_t>(p) * p_items];
+    const int64_t prange = probe_off[p_at + p_items] - probe_off[p_at];
     int64_t items = 0;
     int32_t split = 0;
     if (bc > 0 && pc > 0) {
@@ -111,7 +128,7 @@ __global__ void join_items_kernel(const int64_t* __restrict__ build_off, const i
             split = lg;
             S = 1ll << lg;
         } else {
-            const int64_t brange = build_off[static_cast<int64_t>(p + 1) * b_items] - build_off[static_cast<int64_t>(p) * b_items];
+            const int64_t brange = build_off[b_at + b_items] - build_off[b_at];
             S = (brange + cap_per_table - 1) / cap_per_table;
             if (S < 1) S = 1;
             split = static_cast<int32_t>(S);
@@ -355,7 +372,7 @@ struct JoinSmem {
     }
 };
 
-template <typename K, int TABLE, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF, int THREADS>
+template <typename K, int TABLE, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF, int THREADS, bool BATCH = false>
 __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 {
     using TV = TupleView<K>;
@@ -440,6 +457,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             raise_status(a.status, ST_CAPACITY);
         }
     };
+    JobOut jout{};  // batches: the current item's join
     // Whole warp: every lane appends its c entries; put(stage_index) writes
     // them into the warp's staging buffer.
     auto append = [&](int c, auto&& put) {
@@ -451,6 +469,26 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         }
         const int n = __shfl_sync(0xffffffffu, incl, 31);
         if (n == 0) return;
+        if constexpr (BATCH) {
+            // exact positions in the join's own output: one atomic per warp step
+            unsigned long long q0 = 0;
+            if (lane == 0) q0 = atomicAdd(jout.count, static_cast<unsigned long long>(n));
+            q0 = __shfl_sync(0xffffffffu, q0, 0);
+            if (jout.out_build == nullptr) return;
+            put(incl - c);
+            __syncwarp();
+            for (int i = lane; i < n; i += 32) {
+                const long long pos = static_cast<long long>(q0) + i;
+                if (pos < jout.capacity) {
+                    st_stream(jout.out_build + pos, stage_b[i], stream_pol);
+                    st_stream(jout.out_probe + pos, stage_p[i], stream_pol);
+                } else {
+                    raise_status(a.status, ST_CAPACITY);
+                }
+            }
+            __syncwarp();
+            return;
+        }
         uint32_t q0 = 0;
         if (lane == 0) q0 = atomicAdd(&s_q, static_cast<uint32_t>(n));
         q0 = __shfl_sync(0xffffffffu, q0, 0);
@@ -501,19 +539,31 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         const int64_t piece = local % S;
         const int64_t pchunk = local / S;
         const int sbits = HASH_SPLIT ? split : 0;
-        const int skip = a.digit_bits + sbits;
+        int dbits = a.digit_bits;
+        int64_t b_at = static_cast<int64_t>(p) * a.b_items, p_at = static_cast<int64_t>(p) * a.p_items;
+        int32_t b_n = a.b_items, p_n = a.p_items;
+        if constexpr (BATCH) {
+            const PartRef r = a.parts[p];
+            b_at = r.b_at;
+            p_at = r.p_at;
+            b_n = r.b_items;
+            p_n = r.p_items;
+            dbits = r.digit_bits;
+            jout = a.outs[r.job];
+        }
+        const int skip = dbits + sbits;
         const int piece_shift = 32 - (sbits > 0 ? sbits : 1);
 
-        const int64_t b_lo0 = a.build_off[static_cast<int64_t>(p) * a.b_items];
-        const int64_t b_hi0 = a.build_off[static_cast<int64_t>(p + 1) * a.b_items];
+        const int64_t b_lo0 = a.build_off[b_at];
+        const int64_t b_hi0 = a.build_off[b_at + b_n];
         int64_t b_lo = b_lo0, b_hi = b_hi0;
         if (!HASH_SPLIT) {
             b_lo = b_lo0 + piece * a.position_chunk;
             b_hi = b_lo + a.position_chunk < b_hi0 ? b_lo + a.position_chunk : b_hi0;
             if (b_lo > b_hi) b_lo = b_hi;
         }
-        const int64_t q_lo0 = a.probe_off[static_cast<int64_t>(p) * a.p_items];
-        const int64_t q_hi0 = a.probe_off[static_cast<int64_t>(p + 1) * a.p_items];
+        const int64_t q_lo0 = a.probe_off[p_at];
+        const int64_t q_hi0 = a.probe_off[p_at + p_n];
         const int64_t q_lo = q_lo0 + pchunk * a.probe_chunk;
         const int64_t q_hi = q_lo + a.probe_chunk < q_hi0 ? q_lo + a.probe_chunk : q_hi0;
 
@@ -526,7 +576,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 
         auto in_piece = [&](uint32_t h) -> bool {
             if (!HASH_SPLIT || sbits == 0) return true;
-            return static_cast<int64_t>((h << a.digit_bits) >> piece_shift) == piece;
+            return static_cast<int64_t>((h << dbits) >> piece_shift) == piece;
         };
         auto bucket_of = [&](uint32_t h) -> uint32_t { return h & nb_mask; };
         auto finger_of = [&](uint32_t h) -> uint32_t { return (h >> a.nb_log2) & 0xffffu; };
@@ -659,7 +709,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         // (not for COMPACT or EXACT tables: their 32 K-tuple build ranges were evicted
         // again before use -- 2^27 x 2^27 int32: 0.83 GB more DRAM reads and
         // no time gained, while 16 K-tuple BUCKET ranges gain 8% at 2^25)
-        if (TABLE != TABLE_COMPACT && TABLE != TABLE_EXACT && threadIdx.x == 0 && next_p >= 0 && next_p != p) {
+        if (!BATCH && TABLE != TABLE_COMPACT && TABLE != TABLE_EXACT && threadIdx.x == 0 && next_p >= 0 &&
+            next_p != p) {
             const int64_t nb_lo = a.build_off[static_cast<int64_t>(next_p) * a.b_items];
             const int64_t nb_hi = a.build_off[static_cast<int64_t>(next_p + 1) * a.b_items];
             const int64_t nbytes = (nb_hi - nb_lo) * TV::WORDS * 4;
@@ -1033,7 +1084,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     }
     // ---- record this CTA's entries and last chunk for the fix-up ----
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (!BATCH && threadIdx.x == 0) {
         const uint32_t q = s_q;
         a.cta_q[blockIdx.x] = q;
         a.cta_last[blockIdx.x] =

@@ -33,6 +33,7 @@
 
 #include "pj_device.cuh"
 #include "pj_heavy.cuh"
+#include "pj_types.cuh"
 
 namespace pj {
 
@@ -794,6 +795,87 @@ __global__ void __launch_bounds__(THREADS, 1) scatter_tuples_kernel(const uint32
             wc_place<K, W, VT>(w, dv, ok, buf, cap, fc, out, out_cap, status);
         }
         wc_finish<K, W>(P, buf, cap, fc, out, out_cap, offsets, n_items, item, status);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batches of joins: histogram and scatter over the items (SegItem) of many
+// join sides in one launch each.
+
+// Histogram of the items (grid = items * hsplit, hsplit CTAs per item).
+template <typename K>
+__global__ void __launch_bounds__(HIST_THREADS) hist_seg_kernel(const SegItem* __restrict__ items, int32_t hsplit,
+                                                                uint32_t* __restrict__ counts,
+                                                                int32_t* __restrict__ totals)
+{
+    extern __shared__ __align__(16) uint32_t cnt[];
+    const SegItem it = items[blockIdx.x / hsplit];
+    const int part = blockIdx.x % hsplit;
+    for (int p = threadIdx.x; p < it.P; p += HIST_THREADS) cnt[p] = 0;
+    __syncthreads();
+    const K* keys = static_cast<const K*>(it.keys);
+    const int64_t per = (((it.hi - it.lo) + hsplit - 1) / hsplit + 15) & ~int64_t(15);
+    int64_t s_lo = it.lo + part * per;
+    const int64_t s_hi = s_lo + per < it.hi ? s_lo + per : it.hi;
+    if (s_lo > s_hi) s_lo = s_hi;
+    for (int64_t i = s_lo + threadIdx.x; i < s_hi; i += HIST_THREADS)
+        atomicAdd(&cnt[(hash_key(keys[i]) >> it.f.shift) & it.f.mask], 1u);
+    __syncthreads();
+    for (int p = threadIdx.x; p < it.P; p += HIST_THREADS) {
+        const uint32_t c = cnt[p];
+        if (c) {
+            atomicAdd(&counts[it.cnt_base + static_cast<int64_t>(p) * it.seg_items + it.item], c);
+            atomicAdd(&totals[it.tot_base + p], static_cast<int32_t>(c));
+        }
+    }
+}
+
+// Write-combining scatter of the items (persistent grid; buffers sized for
+// the largest partition count of the batch, Pmax).
+template <typename K, int THREADS, int VT, int W>
+__global__ void __launch_bounds__(THREADS, 1) scatter_seg_kernel(const SegItem* __restrict__ items, int32_t n_items,
+                                                                 int32_t Pmax, int32_t cap,
+                                                                 const int64_t* __restrict__ offsets,
+                                                                 uint32_t* __restrict__ out, uint32_t out_cap,
+                                                                 uint32_t* __restrict__ status)
+{
+    constexpr int TW = WcTraits<K, W>::TW;
+    constexpr int ROUND = THREADS * VT;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
+    const WcState fc = WcState::at(buf + static_cast<size_t>(Pmax) * cap * TW, Pmax);
+    for (int32_t i = blockIdx.x; i < n_items; i += gridDim.x) {
+        const SegItem it = items[i];
+        const int64_t* off = offsets + it.cnt_base;
+        for (int p = threadIdx.x; p < it.P; p += THREADS)
+            fc.init(p, static_cast<int>(off[static_cast<int64_t>(p) * it.seg_items + it.item]));
+        __syncthreads();
+        const K* keys = static_cast<const K*>(it.keys);
+        K nk[VT];
+        auto load_round = [&](int64_t b) {
+#pragma unroll
+            for (int v = 0; v < VT; ++v) {
+                const int64_t r = b + static_cast<int64_t>(v) * THREADS + threadIdx.x;
+                nk[v] = r < it.hi ? keys[r] : K(0);
+            }
+        };
+        if (it.lo < it.hi) load_round(it.lo);
+        for (int64_t b = it.lo; b < it.hi; b += ROUND) {
+            uint32_t w[VT][TW];
+            uint32_t dv[VT];
+            bool ok[VT];
+#pragma unroll
+            for (int v = 0; v < VT; ++v) {
+                const int64_t r = b + static_cast<int64_t>(v) * THREADS + threadIdx.x;
+                ok[v] = r < it.hi;
+                tuple_words<K>(w[v], nk[v], static_cast<int32_t>(r));
+                dv[v] = (tuple_hash<K>(w[v]) >> it.f.shift) & it.f.mask;
+            }
+            if (b + ROUND < it.hi) load_round(b + ROUND);
+            wc_place<K, W, VT>(w, dv, ok, buf, cap, fc, out, out_cap, status);
+        }
+        wc_finish<K, W>(it.P, buf, cap, fc, out, out_cap, off, it.seg_items, it.item, status);
         __syncthreads();
     }
 }

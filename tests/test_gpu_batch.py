@@ -85,3 +85,29 @@ def test_batch_autotune_keeps_results():
     assert c["direct_threads"] in (256, 512, 1024) and 0 <= c["direct_max_build"] <= 40960
     bj.launch()
     _check(bj, host)
+
+
+@pytest.mark.parametrize("dtype", [torch.int32, torch.int64])
+def test_batch_large_joins_run_together(dtype):
+    # joins of 2^18..2^20 build rows: partitioned by one histogram, scan and
+    # scatter launch over all of them and joined by one persistent launch;
+    # the same batch run one join after another must give the same pairs
+    pairs, host = _batch(65, 10, dtype, 18, 20)
+    for together in (1, 0):
+        bj = api.BatchJoiner(pairs)
+        bj.config.large_batched = together
+        bj.prepare()
+        bj.launch()
+        _check(bj, host)
+
+
+def test_batch_large_joins_repeated_keys_and_graph():
+    pairs, host = _batch(66, 12, torch.int32, 15, 18, unique=False)
+    bj = api.BatchJoiner(pairs, unique_build_keys=False)
+    bj.config.direct_max_build = 0  # every join partitioned, all together
+    bj.prepare()
+    g = bj.graph()
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        _check(bj, host, unique=False)
