@@ -50,7 +50,9 @@ def parse_args():
                     help="cfg2: 2^27 x 2^27 int32 uniform (the headline); cfg3: 2^26 x 2^28 int64, Zipf probe "
                          "keys; cfg4: learned against exact plans on a held-out sweep; cfg5: 512 int32 joins of "
                          "uneven sizes, batched against one after another")
-    ap.add_argument("--sweep", type=int, default=80, help="cfg4: held-out workloads")
+    ap.add_argument("--sweep", type=int, default=60, help="cfg4: held-out workloads")
+    ap.add_argument("--cfg4-max-log2-build", type=int, default=28)
+    ap.add_argument("--cfg4-max-log2-probe", type=int, default=29)
     ap.add_argument("--batch", type=int, default=512, help="cfg5: joins in the batch")
     ap.add_argument("--zipf", type=float, default=1.0, help="cfg3: Zipf exponent of the probe keys")
     ap.add_argument("--log2-build", type=int, default=None)
@@ -544,8 +546,10 @@ def run_batch(args, rank, world, local):
     """cfg5: a batch of int32 joins, build sizes log-uniform in 2^10..2^20
     (unique keys), probe sizes 4x, 70 % uniform matches, every fourth join
     with Zipf(1.0) probe keys -- run one after another with the plain
-    method, then as one batch (default, autotuned, autotuned in a CUDA
-    graph).  value = batch input tuples/s of the fastest batched form."""
+    method (default plans, and per-join autotuned plans: the fastest of the
+    default, the exact-histogram plan and one radix bit less or more), then
+    as one batch (default, autotuned, autotuned in a CUDA graph).  value =
+    batch input tuples/s of the fastest batched form."""
     import ctypes
 
     import numpy as np
@@ -612,6 +616,49 @@ def run_batch(args, rank, world, local):
     _lib.check(L.pj_check(ctypes.c_void_p(ws.data_ptr()), None))
     plain_ok = verify_all(keep[0::2], keep[1::2], counts)
 
+    # plain autotuned: every join alone with the fastest of its default plan,
+    # the exact-histogram plan and the default radix width -1 / +1 bit
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def one_ms(d, pl, o, wsb, wsz):
+        _lib.check(L.pj_inner_join(ctypes.byref(d), ctypes.byref(pl), ctypes.byref(o), ctypes.c_void_p(wsb), wsz,
+                                   api._stream_ptr(None)))
+        best = float("inf")
+        for _ in range(2):
+            e0.record(stream)
+            L.pj_inner_join(ctypes.byref(d), ctypes.byref(pl), ctypes.byref(o), ctypes.c_void_p(wsb), wsz,
+                            api._stream_ptr(None))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    tuned_plans = []
+    for (b, p), d, pl, o in zip(pairs, descs, plans, outs):
+        cands = [pl, api.plan_exact(b, p, True)]
+        for dlt in (-1, 1):
+            q = _lib.Plan.from_buffer_copy(pl)
+            q.bits1 = max(0, pl.bits1 + dlt)
+            n = ctypes.c_size_t()
+            if L.pj_workspace_size(ctypes.byref(d), ctypes.byref(q), ctypes.byref(n)) == _lib.OK:
+                cands.append(q)
+        sized = [(c, api.workspace_size(d, c)) for c in cands]
+        tws = api.alloc_workspace(max(z for _, z in sized), device)
+        times = [one_ms(d, c, o, tws.data_ptr(), tws.numel()) for c, _ in sized]
+        tuned_plans.append(cands[int(np.argmin(times))])
+        del tws
+    tws_bytes = max(api.workspace_size(d, pl) for d, pl in zip(descs, tuned_plans))
+    tws = api.alloc_workspace(tws_bytes, device)
+
+    def plain_tuned():
+        for d, pl, o in zip(descs, tuned_plans, outs):
+            _lib.check(L.pj_inner_join(ctypes.byref(d), ctypes.byref(pl), ctypes.byref(o),
+                                       ctypes.c_void_p(tws.data_ptr()), tws_bytes, api._stream_ptr(None)))
+
+    plain_tuned_ms = timed(plain_tuned, steps)
+    _lib.check(L.pj_check(ctypes.c_void_p(tws.data_ptr()), None))
+    plain_tuned_ok = verify_all(keep[0::2], keep[1::2], counts)
+
     bj = api.BatchJoiner(pairs)
     default_cfg = bj.config.as_dict()
     batch_ms = timed(bj.launch, steps)
@@ -631,10 +678,15 @@ def run_batch(args, rank, world, local):
         "config": {"workload": f"{args.batch} int32 joins, build log-uniform 2^10..2^20 unique, probe 4x, 70% "
                                f"matches, every fourth Zipf(1.0) (generated on the device)",
                    "input_tuples": tuples, "batch_default_config": default_cfg, "batch_tuned_config": bj.config.as_dict()},
-        "makespan_ms": {"one_after_another_plain": plain_ms, "batch_default": batch_ms, "batch_autotuned": tuned_ms,
+        "makespan_ms": {"one_after_another_plain": plain_ms, "one_after_another_plain_autotuned": plain_tuned_ms,
+                        "batch_default": batch_ms, "batch_autotuned": tuned_ms,
                         "batch_autotuned_graph": graph_ms, "autotuner_estimate": tuned_ms_est},
         "speedup_vs_plain": plain_ms / best_ms,
-        "verified": {"plain": plain_ok, "batch": batch_ok, "graph": graph_ok},
+        "speedup_vs_plain_autotuned": plain_tuned_ms / best_ms,
+        "joins_by_path": {"direct": int(sum(1 for b, _ in pairs if 0 < b.numel() <= bj.config.direct_max_build)),
+                          "partitioned_together": int(sum(1 for b, _ in pairs if b.numel() > bj.config.direct_max_build))
+                          if bj.config.large_batched else 0},
+        "verified": {"plain": plain_ok, "plain_autotuned": plain_tuned_ok, "batch": batch_ok, "graph": graph_ok},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -642,8 +694,9 @@ def run_batch(args, rank, world, local):
 
 def run_learned(args, rank, world, local):
     """cfg4: the shipped planner weights against the exact-histogram planner
-    on a held-out seeded sweep (build 2^14..2^24 log-uniform, probe/build 1,
-    4 or 16, int32 or int64, Zipf 0..1.5, match rate 0.1..1).  Per workload
+    on a held-out seeded sweep (build 2^18..2^28 log-uniform, probe/build 1,
+    4 or 16 with the probe side capped at 2^29 rows, int32 or int64, Zipf
+    0..1.5, match rate 0.1..1).  Per workload
     both plans are made and timed (join time, and planning time apart);
     value = geometric-mean speedup of the learned plans' joins, fallbacks
     (a learned plan that overflows, rerun with the exact plan) counted at
@@ -675,7 +728,7 @@ def run_learned(args, rank, world, local):
         return best, st
 
     for i in range(args.sweep):
-        b, p, meta = planner.sweep_workload(rng, 24, 26)
+        b, p, meta = planner.sweep_workload(rng, args.cfg4_max_log2_build, args.cfg4_max_log2_probe)
         t0 = time.perf_counter()
         exact = api.plan_exact(b, p, True)
         plan_exact_ms = 1e3 * (time.perf_counter() - t0)
@@ -702,8 +755,9 @@ def run_learned(args, rank, world, local):
         "metric": "geomean speedup of learned over exact plans (cfg4 held-out sweep)", "value": geo, "unit": "x",
         "n_gpus": world, "steps": 2, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/int64", "data": "synthetic",
-        "config": {"workload": f"{args.sweep} held-out joins: build 2^14..2^24 log-uniform, probe/build 1/4/16, "
-                               "int32 or int64, Zipf 0..1.5, match 0.1..1 (generated on the device)"},
+        "config": {"workload": f"{args.sweep} held-out joins: build 2^18..2^{args.cfg4_max_log2_build} log-uniform, "
+                               f"probe/build 1/4/16 (at most 2^{args.cfg4_max_log2_probe}), int32 or int64, Zipf 0..1.5, "
+                               "match 0.1..1 (generated on the device)"},
         "fallback_rate": float(np.mean([r["fallback"] for r in rows])),
         "speedup_by_zipf": {"uniform(<0.2)": geo_of(z < 0.2), "0.2-1.0": geo_of((z >= 0.2) & (z < 1.0)),
                             ">=1.0": geo_of(z >= 1.0)},

@@ -354,15 +354,18 @@ pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, in
                             size_t workspace_bytes, pj_stream stream, pj_batch_config* best, float* best_ms);
 
 /* ---- learned planner (no reference counterpart) ----------------------------
- * A small MLP ranks PJ_PLAN_CANDIDATES schedules of a join -- table layout
- * (BUCKET or COMPACT) x radix bits (the default -1, 0, +1) x heavy-key path
- * (off, on) -- from a sketch of a probe-key sample and the sizes.  It only
+ * A small MLP ranks PJ_PLAN_CANDIDATES schedules of a join -- one radix
+ * pass with BUCKET, COMPACT or EXACT tables x radix bits (the layout's own
+ * width -1, 0, +1) x heavy-key set (none, every heavy key of the probe
+ * sample, its 16 most frequent), and two radix passes with BUCKET tables at
+ * the width +0, +1, +2 -- from a sketch of a probe-key sample and the
+ * sizes.  It only
  * chooses the schedule: results are those of any plan, and a choice that
  * overflows a table on the device is rerun with pj_plan_exact by the caller
  * (PJ_ERR_OVERFLOW from pj_check). */
 #define PJ_MLP_FEATURES 32
 #define PJ_MLP_HIDDEN 64
-#define PJ_PLAN_CANDIDATES 12
+#define PJ_PLAN_CANDIDATES 30
 
 /* Shape of an MLP: in -> h1 (ReLU) -> h2 (ReLU) -> out.  Parameters are one
  * float vector W1[in][h1], b1, W2[h1][h2], b2, W3[h2][out], b3. */

@@ -70,7 +70,7 @@ class MlpDims(ctypes.Structure):
     _fields_ = [("in_", ctypes.c_int32), ("h1", ctypes.c_int32), ("h2", ctypes.c_int32), ("out", ctypes.c_int32)]
 
 
-MLP_FEATURES, MLP_HIDDEN, PLAN_CANDIDATES = 32, 64, 12  # PJ_MLP_FEATURES, PJ_MLP_HIDDEN, PJ_PLAN_CANDIDATES
+MLP_FEATURES, MLP_HIDDEN, PLAN_CANDIDATES = 32, 64, 30  # PJ_MLP_FEATURES, PJ_MLP_HIDDEN, PJ_PLAN_CANDIDATES
 
 
 # every symbol include/pj.h declares, with its ctypes signature

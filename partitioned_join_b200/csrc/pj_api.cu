@@ -1506,20 +1506,59 @@ pj_status pj_plan_candidate(const pj_join_desc* d, int32_t candidate, const pj_p
     pj_plan p;
     pj_status s = pj_plan_default(d, &p);
     if (s != PJ_OK) return s;
-    const int table = candidate / 6, delta = (candidate % 6) / 2 - 1, heavy_on = candidate % 2;
-    p.table_mode = table ? PJ_TABLE_COMPACT : PJ_TABLE_BUCKET;
-    p.table_capacity = max_table_capacity(d->key_bytes, p.table_mode);
+    p.n_heavy = 0;
     int max_bits = 0;
     for (int b = 0; b <= 16; ++b)
         if (pick_wc(d->key_bytes, b) != 0) max_bits = b;
-    const int bits = std::min(std::max(bits_for_table(d->n_build, p.table_capacity) + delta, 0), max_bits);
-    p.bits1 = bits;
-    p.wc_tuples = pick_wc(d->key_bytes, bits);
-    if (p.wc_tuples == 0) return PJ_ERR_INVALID;
-    p.n_heavy = 0;
-    if (heavy_on && heavy && d->unique_build_keys && heavy->n_heavy > 0) {
-        p.n_heavy = std::min(heavy->n_heavy, PJ_MAX_HEAVY);
-        for (int i = 0; i < p.n_heavy; ++i) p.heavy_keys[i] = heavy->heavy_keys[i];
+    const double n = static_cast<double>(std::max<int64_t>(d->n_build, 1));
+    auto largest = [&](int bits) {  // expected largest hashed partition: mean + 4 standard deviations
+        const double m = n / static_cast<double>(int64_t(1) << bits);
+        return m + 4.0 * std::sqrt(m) + 1.0;
+    };
+    if (candidate < 27) {
+        // table layout x radix bits (-1, 0, +1 around the layout's own width) x heavy-key set
+        const int table = candidate / 9, delta = (candidate % 9) / 3 - 1, heavy_mode = candidate % 3;
+        p.digit_mode = PJ_DIGIT_HASH;
+        p.split_mode = d->unique_build_keys ? PJ_SPLIT_HASH : PJ_SPLIT_POSITION;
+        if (table == 0 || table == 1) {
+            p.table_mode = table == 0 ? PJ_TABLE_BUCKET : PJ_TABLE_COMPACT;
+            p.table_capacity = max_table_capacity(d->key_bytes, p.table_mode);
+            // (a COMPACT choice whose partitions exceed an entry's 65536-tuple
+            // index range is valid here and overflows on the device: the
+            // caller then falls back to the exact plan)
+            p.bits1 = std::min(std::max(bits_for_table(d->n_build, p.table_capacity) + delta, 0), max_bits);
+        } else {
+            // EXACT: hash digits and enough buckets that an entry fixes the key
+            const int ccap = max_table_capacity(d->key_bytes, PJ_TABLE_COMPACT);
+            p.bits1 = std::min(std::max(bits_for_table(d->n_build, ccap) + delta, 0), max_bits);
+            const int cap_e = exact_table_capacity(d->key_bytes, exact_row_bits(d->n_build) - p.bits1);
+            if (cap_e == 0 || largest(p.bits1) > cap_e) return PJ_ERR_INVALID;
+            p.table_mode = PJ_TABLE_EXACT;
+            p.table_capacity = cap_e;
+            if (!d->unique_build_keys) return PJ_ERR_INVALID;
+        }
+        p.wc_tuples = pick_wc(d->key_bytes, p.bits1);
+        if (p.wc_tuples == 0) return PJ_ERR_INVALID;
+        if (heavy_mode != 0) {
+            // the sample's heavy keys (most frequent first): all of them, or the 16 most frequent
+            if (!heavy || !d->unique_build_keys || heavy->n_heavy <= 0) return PJ_ERR_INVALID;
+            p.n_heavy = std::min(heavy_mode == 1 ? heavy->n_heavy : std::min(heavy->n_heavy, 16), PJ_MAX_HEAVY);
+            for (int i = 0; i < p.n_heavy; ++i) p.heavy_keys[i] = heavy->heavy_keys[i];
+            if (p.table_mode == PJ_TABLE_EXACT) return PJ_ERR_INVALID;  // the heavy path keeps COMPACT/BUCKET tables
+        }
+    } else {
+        // two radix passes, BUCKET tables: the BUCKET width + 0, 1 or 2 bits, split evenly
+        p.table_mode = PJ_TABLE_BUCKET;
+        p.digit_mode = PJ_DIGIT_HASH;
+        p.table_capacity = max_table_capacity(d->key_bytes, PJ_TABLE_BUCKET);
+        const int bits = bits_for_table(d->n_build, p.table_capacity) + (candidate - 27);
+        if (bits < 2) return PJ_ERR_INVALID;
+        p.passes = 2;
+        p.bits1 = (bits + 1) / 2;
+        p.bits2 = bits - p.bits1;
+        p.wc_tuples = pick_wc(d->key_bytes, p.bits1);
+        if (p.wc_tuples == 0 || pass2_wc(d->key_bytes, &p) == 0) return PJ_ERR_INVALID;
+        p.split_mode = d->unique_build_keys ? PJ_SPLIT_HASH : PJ_SPLIT_POSITION;
     }
     if ((s = check_plan(d, &p)) != PJ_OK) return s;
     *plan = p;

@@ -1,10 +1,11 @@
 """Learned planner: an MLP that ranks candidate schedules of a join.
 
-The network (PJ_MLP_FEATURES -> 64 -> 64 -> PJ_PLAN_CANDIDATES, ~7 K FP32
+The network (PJ_MLP_FEATURES -> 64 -> 64 -> PJ_PLAN_CANDIDATES, ~8 K FP32
 weights) reads a sketch of a probe-key sample plus the sizes
-(pj_plan_features) and predicts, for each candidate schedule (table layout x
-radix bits x heavy-key path, pj_plan_candidate), its run time relative to
-the others (log2 ms minus the workload's mean).  It is trained on the GPU by
+(pj_plan_features) and predicts, for each candidate schedule (one pass with
+BUCKET, COMPACT or EXACT tables x radix bits x heavy-key set, or two passes,
+pj_plan_candidate), its run time relative to the others (log2 ms minus the
+workload's mean).  It is trained on the GPU by
 the library's own kernels (pj_mlp_forward / pj_mlp_backward /
 pj_mlp_mse_grad / pj_mlp_adam) on timings that the plain method generates
 over a seeded synthetic sweep.  The exact-histogram planner (pj_plan_exact)
@@ -194,11 +195,14 @@ def _time_join(desc, plan, ws, nb, out, reps=2) -> (float, int):
     return best, status
 
 
-def sweep_workload(rng: np.random.Generator, max_log2_build=22, max_log2_probe=25, device="cuda"):
+def sweep_workload(rng: np.random.Generator, max_log2_build=28, max_log2_probe=29, device="cuda",
+                   min_log2_build=18):
     """One seeded workload of the planner sweep: build rows log-uniform in
-    2^14..2^max, probe/build ratio 1, 4 or 16, int32 or int64 keys, Zipf
-    exponent uniform in [0, 1.5] (0 below 0.2), match rate in [0.1, 1]."""
-    lb = rng.uniform(14, max_log2_build)
+    2^min..2^max, probe/build ratio 1, 4 or 16 (the probe side capped at
+    2^max_log2_probe rows: row ids are int32, and a 2^28 x 2^32 join would
+    need about 100 GB of workspace), int32 or int64 keys, Zipf exponent
+    uniform in [0, 1.5] (0 below 0.2), match rate in [0.1, 1]."""
+    lb = rng.uniform(min_log2_build, max_log2_build)
     nb = int(2 ** lb)
     ratio = int(rng.choice([1, 4, 16]))
     np_ = min(nb * ratio, 1 << max_log2_probe)
@@ -242,8 +246,15 @@ def measure(build, probe):
     return feat, times, failed, t_exact
 
 
-def targets(times: np.ndarray):
-    """Relative log2 times (minus the workload's mean) and the valid mask."""
+def targets(times: np.ndarray, failed: Optional[np.ndarray] = None, t_exact: Optional[np.ndarray] = None):
+    """Relative log2 times (minus the workload's mean) and the mask of the
+    candidates that carry a target.  A candidate that overflowed on the
+    device costs its run plus the exact plan's (what choosing it costs), so
+    the network learns to avoid it; candidates that could not be built are
+    masked out."""
+    if failed is not None and t_exact is not None:
+        ran_out = np.isnan(times) & (failed > 0)
+        times = np.where(ran_out, failed + t_exact[:, None], times)
     lt = np.log2(np.where(np.isnan(times), 1.0, times))
     mask = (~np.isnan(times)).astype(np.float32)
     mean = (lt * mask).sum(1, keepdims=True) / np.maximum(mask.sum(1, keepdims=True), 1)
@@ -275,8 +286,9 @@ def main():
     ap.add_argument("--held-out", type=float, default=0.25)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--seed", type=int, default=11)
-    ap.add_argument("--max-log2-build", type=int, default=22)
-    ap.add_argument("--max-log2-probe", type=int, default=25)
+    ap.add_argument("--min-log2-build", type=int, default=18)
+    ap.add_argument("--max-log2-build", type=int, default=28)
+    ap.add_argument("--max-log2-probe", type=int, default=29)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--data", default="", help="save the sweep (npz) here")
     a = ap.parse_args()
@@ -284,14 +296,14 @@ def main():
     F, T, FAIL, TEX, META = [], [], [], [], []
     t0 = time.time()
     for i in range(a.workloads):
-        b, p, meta = sweep_workload(rng, a.max_log2_build, a.max_log2_probe)
+        b, p, meta = sweep_workload(rng, a.max_log2_build, a.max_log2_probe, min_log2_build=a.min_log2_build)
         f, t, fl, te = measure(b, p)
         F.append(f), T.append(t), FAIL.append(fl), TEX.append(te), META.append(meta)
         del b, p
     F, T, FAIL, TEX = (np.array(x) for x in (F, T, FAIL, TEX))
     if a.data:
         np.savez(a.data, features=F, times=T, failed=FAIL, t_exact=TEX, meta=json.dumps(META))
-    tgt, mask = targets(T)
+    tgt, mask = targets(T, FAIL, TEX)
     n_test = int(round(a.held_out * len(F)))
     tr, te = slice(n_test, None), slice(0, n_test)
     net = Mlp(seed=a.seed)
@@ -299,8 +311,9 @@ def main():
     report = {"train": evaluate(net.predict(F[tr]), T[tr], FAIL[tr], TEX[tr]),
               "held_out": evaluate(net.predict(F[te]), T[te], FAIL[te], TEX[te]),
               "loss_first_last": [losses[0], losses[-1]], "sweep_seconds": time.time() - t0,
-              "sweep": {"workloads": a.workloads, "seed": a.seed, "max_log2_build": a.max_log2_build,
-                        "max_log2_probe": a.max_log2_probe}}
+              "sweep": {"workloads": a.workloads, "seed": a.seed, "min_log2_build": a.min_log2_build,
+                        "max_log2_build": a.max_log2_build, "max_log2_probe": a.max_log2_probe},
+        "candidates": _lib.PLAN_CANDIDATES}
     np.savez(a.out, params=net.params.cpu().numpy(), report=json.dumps(report))
     print(json.dumps(report))
 
