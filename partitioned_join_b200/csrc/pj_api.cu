@@ -1773,11 +1773,13 @@ pj_status large_batch_layout(const pj_join_desc* descs, const std::vector<int>& 
             r.digit_bits = j.bits;
             lb.parts.push_back(r);
         }
-        // work items: each partition's hash pieces times its probe chunks
-        const int64_t max_pieces = static_cast<int64_t>(P) << MAX_SPLIT_LOG2;
-        max_items += std::min<int64_t>(max_pieces * (P + part_capacity(d.n_probe, P, nit[1], lb.W) / lb.probe_chunk + 1),
-                                       static_cast<int64_t>(P) * 4096 + max_pieces + P +
-                                           part_capacity(d.n_probe, P, nit[1], lb.W) / lb.probe_chunk + 1);
+        // work items: each partition's build pieces (hash pieces, or
+        // table-sized position pieces) times its probe chunks, as make_layout
+        const int64_t per_piece = std::max<int64_t>(16, lb.table_cap / 16 * 16);
+        const int64_t max_pieces = std::max<int64_t>(static_cast<int64_t>(P) << MAX_SPLIT_LOG2,
+                                                     P + part_capacity(d.n_build, P, nit[0], lb.W) / per_piece);
+        const int64_t max_chunks = P + part_capacity(d.n_probe, P, nit[1], lb.W) / lb.probe_chunk + 1;
+        max_items += std::min<int64_t>(max_pieces * max_chunks, static_cast<int64_t>(P) * 4096 + max_pieces + max_chunks);
         lb.joins.push_back(j.idx);
         g += P;
     }
