@@ -357,8 +357,9 @@ pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, in
  * A small MLP ranks PJ_PLAN_CANDIDATES schedules of a join -- one radix
  * pass with BUCKET, COMPACT or EXACT tables x radix bits (the layout's own
  * width -1, 0, +1) x heavy-key set (none, every heavy key of the probe
- * sample, its 16 most frequent), and two radix passes with BUCKET tables at
- * the width +0, +1, +2 -- from a sketch of a probe-key sample and the
+ * sample, its 16 most frequent), two radix passes with BUCKET tables at
+ * the width +0 and +1, and the exact-histogram planner's own plan
+ * (PJ_PLAN_CANDIDATE_EXACT) -- from a sketch of a probe-key sample and the
  * sizes.  It only
  * chooses the schedule: results are those of any plan, and a choice that
  * overflows a table on the device is rerun with pj_plan_exact by the caller
@@ -366,6 +367,7 @@ pj_status pj_batch_autotune(const pj_join_desc* descs, const pj_output* outs, in
 #define PJ_MLP_FEATURES 32
 #define PJ_MLP_HIDDEN 64
 #define PJ_PLAN_CANDIDATES 30
+#define PJ_PLAN_CANDIDATE_EXACT 29  /* the last candidate: pj_plan_exact's plan */
 
 /* Shape of an MLP: in -> h1 (ReLU) -> h2 (ReLU) -> out.  Parameters are one
  * float vector W1[in][h1], b1, W2[h1][h2], b2, W3[h2][out], b3. */
@@ -405,7 +407,8 @@ pj_status pj_plan_features(const pj_join_desc* desc, void* workspace, size_t wor
 
 /* Candidate schedule c (0 .. PJ_PLAN_CANDIDATES-1) from the sizes and a heavy
  * set (from pj_plan_features; NULL: none).  PJ_ERR_INVALID if c cannot be
- * built for this join. */
+ * built for this join, and for PJ_PLAN_CANDIDATE_EXACT, which needs the
+ * device (pj_plan_exact). */
 pj_status pj_plan_candidate(const pj_join_desc* desc, int32_t candidate, const pj_plan* heavy, pj_plan* plan);
 
 /* Learned plan: features, the MLP (params: device, PJ_MLP_FEATURES ->

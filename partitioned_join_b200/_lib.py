@@ -71,6 +71,7 @@ class MlpDims(ctypes.Structure):
 
 
 MLP_FEATURES, MLP_HIDDEN, PLAN_CANDIDATES = 32, 64, 30  # PJ_MLP_FEATURES, PJ_MLP_HIDDEN, PJ_PLAN_CANDIDATES
+PLAN_CANDIDATE_EXACT = 29  # PJ_PLAN_CANDIDATE_EXACT
 
 
 # every symbol include/pj.h declares, with its ctypes signature

@@ -396,7 +396,8 @@ int run(Options& o)
         combined_histo_elapsed_ms = hist_ms;
         partition_one_elapsed_ms -= hist_ms;
     }
-    const float partition_two_elapsed_ms = ms[PJ_STAGE_BUILD_PASS2] + ms[PJ_STAGE_PROBE_PASS2];
+    // (a one-pass plan's empty pass-two stages hold only the events' own gap)
+    const float partition_two_elapsed_ms = plan.passes == 2 ? ms[PJ_STAGE_BUILD_PASS2] + ms[PJ_STAGE_PROBE_PASS2] : 0.0f;
     const float data_skew_handle_elapsed_ms = ms[PJ_STAGE_JOIN_PLAN];
     const float join_elapsed_ms = ms[PJ_STAGE_JOIN];
     const float total_elapsed_ms = ms[PJ_STAGE_TOTAL];

@@ -1546,8 +1546,10 @@ pj_status pj_plan_candidate(const pj_join_desc* d, int32_t candidate, const pj_p
             for (int i = 0; i < p.n_heavy; ++i) p.heavy_keys[i] = heavy->heavy_keys[i];
             if (p.table_mode == PJ_TABLE_EXACT) return PJ_ERR_INVALID;  // the heavy path keeps COMPACT/BUCKET tables
         }
+    } else if (candidate == PJ_PLAN_CANDIDATE_EXACT) {
+        return PJ_ERR_INVALID;  // pj_plan_exact's plan: made on the device by pj_plan_learned
     } else {
-        // two radix passes, BUCKET tables: the BUCKET width + 0, 1 or 2 bits, split evenly
+        // two radix passes, BUCKET tables: the BUCKET width + 0 or 1 bit, split evenly
         p.table_mode = PJ_TABLE_BUCKET;
         p.digit_mode = PJ_DIGIT_HASH;
         p.table_capacity = max_table_capacity(d->key_bytes, PJ_TABLE_BUCKET);
@@ -1592,8 +1594,10 @@ pj_status pj_plan_learned(const pj_join_desc* d, const float* params, void* ws, 
     int order[PJ_PLAN_CANDIDATES];
     for (int i = 0; i < PJ_PLAN_CANDIDATES; ++i) order[i] = i;
     std::sort(order, order + PJ_PLAN_CANDIDATES, [&](int a, int b) { return out[a] < out[b]; });
-    for (int c : order)
+    for (int c : order) {
+        if (c == PJ_PLAN_CANDIDATE_EXACT) return pj_plan_exact(d, ws, ws_bytes, plan, stream);
         if (pj_plan_candidate(d, c, &heavy, plan) == PJ_OK) return PJ_OK;
+    }
     return pj_plan_default(d, plan);
 }
 

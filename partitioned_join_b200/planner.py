@@ -222,6 +222,7 @@ def measure(build, probe):
     d = api.make_desc(build, probe, True)
     cands = [candidate(build, probe, c, heavy) for c in range(_lib.PLAN_CANDIDATES)]
     exact = api.plan_exact(build, probe, True)
+    cands[_lib.PLAN_CANDIDATE_EXACT] = None  # timed below as the exact plan
     plans = [p for p in cands if p is not None] + [exact]
     nb = _ws_for(d, plans)
     ws = api.alloc_workspace(nb, build.device)
@@ -243,6 +244,7 @@ def measure(build, probe):
             failed[c] = t
     t_exact, st = _time_join(d, exact, ws, nb, out)
     check(st, "exact plan")
+    times[_lib.PLAN_CANDIDATE_EXACT] = t_exact
     return feat, times, failed, t_exact
 
 
@@ -262,10 +264,12 @@ def targets(times: np.ndarray, failed: Optional[np.ndarray] = None, t_exact: Opt
 
 
 def evaluate(pred: np.ndarray, times: np.ndarray, failed: np.ndarray, t_exact: np.ndarray):
-    """Learned choice (argmin prediction) against the exact plan, per
-    workload: the chosen candidate's time, or, when it overflowed, that run
-    plus the exact plan's (the fallback)."""
-    choice = pred.argmin(1)
+    """Learned choice against the exact plan, per workload: the best-ranked
+    candidate that can be built (as pj_plan_learned picks it), its time, or,
+    when it overflowed on the device, that run plus the exact plan's (the
+    fallback)."""
+    buildable = ~np.isnan(times) | (failed > 0)
+    choice = np.where(buildable, pred, np.inf).argmin(1)
     rows = np.arange(pred.shape[0])
     t = times[rows, choice]
     fb = np.isnan(t)

@@ -157,7 +157,7 @@ def test_shipped_weights_gain_over_exact_plans():
             t = min(t, e0.elapsed_time(e1))
         return t, st
 
-    for _ in range(12):
+    for _ in range(20):
         b, p, meta = planner.sweep_workload(rng, 24, 26, min_log2_build=20)
         exact = api.plan_exact(b, p, True)
         t_exact, st = best_ms(api.Joiner(b, p, True, exact))
