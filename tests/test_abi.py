@@ -98,3 +98,30 @@ def test_plan_radix_follows_the_reference_flags(L):
     for bad in ((100, 0, 3.0), (256, 100, 3.0), (256, 0, 0.0), (0, 0, 3.0)):
         assert L.pj_plan_radix(ctypes.byref(d), bad[0], bad[1], ctypes.c_float(bad[2]), ctypes.byref(p)) == \
             _lib.ERR_INVALID, bad
+
+
+def test_plan_candidates_cover_the_schedule_space(L):
+    """pj_plan_candidate: one pass with BUCKET/COMPACT/EXACT tables x radix
+    width -1/0/+1 x heavy set (none/all/16 most frequent), two passes, and
+    the exact planner's plan (made on the device, so not built here)."""
+    from partitioned_join_b200 import _lib, api
+    d = api.desc_for_sizes(1 << 24, 1 << 24, 4)
+    heavy = _lib.Plan()
+    heavy.set_heavy(range(100, 140))
+    modes = {}
+    for c in range(_lib.PLAN_CANDIDATES):
+        p = _lib.Plan()
+        st = L.pj_plan_candidate(ctypes.byref(d), c, ctypes.byref(heavy), ctypes.byref(p))
+        if c == _lib.PLAN_CANDIDATE_EXACT:
+            assert st == _lib.ERR_INVALID
+            continue
+        if st != _lib.OK:
+            continue
+        modes[c] = (p.passes, p.table_mode, p.bits1, p.n_heavy)
+    assert any(m[1] == _lib.TABLE_BUCKET for m in modes.values())
+    assert any(m[1] == _lib.TABLE_COMPACT for m in modes.values())
+    assert any(m[1] == _lib.TABLE_EXACT for m in modes.values())
+    assert any(m[0] == 2 for m in modes.values())
+    assert {m[3] for m in modes.values()} >= {0, 16, 40}
+    # the three radix widths of one layout differ by one bit each
+    assert modes[0][2] + 1 == modes[3][2] and modes[3][2] + 1 == modes[6][2]
