@@ -520,6 +520,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         __syncwarp();
     };
 
+    bool first_item = true;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -567,6 +568,13 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         const int64_t q_lo = q_lo0 + pchunk * a.probe_chunk;
         const int64_t q_hi = q_lo + a.probe_chunk < q_hi0 ? q_lo + a.probe_chunk : q_hi0;
 
+        // a CTA's first item: its build range was not prefetched during an
+        // earlier probe phase
+        if (TABLE != TABLE_COMPACT && first_item && threadIdx.x == 0 && b_hi > b_lo) {
+            const int64_t bbytes = (b_hi - b_lo) * TV::WORDS * 4;
+            prefetch_l2(a.build_tuples + b_lo * TV::WORDS, bbytes < (1 << 20) ? bbytes : (1 << 20));
+        }
+        first_item = false;
         // the head of the probe chunk streams into L2 while the table is built
         if (threadIdx.x == 0) {
             const int64_t pbytes = (q_hi - q_lo) * TV::WORDS * 4;
@@ -705,14 +713,21 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             __syncthreads();
         }
 
-        // the next item's build side streams into L2 while this item probes
-        // (not for COMPACT or EXACT tables: their 32 K-tuple build ranges were evicted
-        // again before use -- 2^27 x 2^27 int32: 0.83 GB more DRAM reads and
-        // no time gained, while 16 K-tuple BUCKET ranges gain 8% at 2^25)
-        if (!BATCH && TABLE != TABLE_COMPACT && TABLE != TABLE_EXACT && threadIdx.x == 0 && next_p >= 0 &&
-            next_p != p) {
-            const int64_t nb_lo = a.build_off[static_cast<int64_t>(next_p) * a.b_items];
-            const int64_t nb_hi = a.build_off[static_cast<int64_t>(next_p + 1) * a.b_items];
+        // the next item's build side streams into L2 while this item probes,
+        // so the next build's count pass reads L2 (BUCKET tables: 8% at
+        // 2^25; EXACT tables: 2^27 x 2^27 int32 join 1.72 -> 1.59 ms).  Not
+        // for COMPACT tables: their fingerprint checks re-read build tuples
+        // and the prefetched ranges were evicted before use (0.83 GB more
+        // DRAM reads at 2^27 x 2^27, no time gained).
+        if (TABLE != TABLE_COMPACT && threadIdx.x == 0 && next_p >= 0 && next_p != p) {
+            int64_t nb_at = static_cast<int64_t>(next_p) * a.b_items;
+            int32_t nb_n = a.b_items;
+            if constexpr (BATCH) {
+                nb_at = a.parts[next_p].b_at;
+                nb_n = a.parts[next_p].b_items;
+            }
+            const int64_t nb_lo = a.build_off[nb_at];
+            const int64_t nb_hi = a.build_off[nb_at + nb_n];
             const int64_t nbytes = (nb_hi - nb_lo) * TV::WORDS * 4;
             prefetch_l2(a.build_tuples + nb_lo * TV::WORDS, nbytes < (1 << 20) ? nbytes : (1 << 20));
         }
@@ -911,45 +926,40 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                     });
                 } else if constexpr (UNIQUE && TABLE == TABLE_EXACT) {
                     // every tuple matches at most once, and an entry's bits decide
-                    // it: the U tuples walk their buckets in lockstep, no loads
-                    bool emit[U], live[U];
+                    // it.  Predicated walk: each pass looks at one entry of every
+                    // unfinished tuple, selects instead of branches, and the loop
+                    // runs while any lane has one left (2^27 x 2^27 int32 join
+                    // 1.72 -> 1.53 ms against a branchy lockstep walk)
+                    bool emit[U];
                     uint32_t brow[U], fq[U];
                     int at[U], end[U];
+                    const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
                         emit[u] = false;
                         brow[u] = 0;
                         fq[u] = xfinger_of(h[u]);
-                        live[u] = r[u] >= 0 && in_piece(h[u]);
-                        at[u] = end[u] = 0;
-                        if (live[u]) {
-                            const uint32_t b = bucket_of(h[u]);
-                            const uint32_t wb = ends[b >> 1];
-                            const uint32_t wa = b == 0 ? 0u : ends[(b - 1) >> 1];
-                            end[u] = static_cast<int>((wb >> ((b & 1u) * 16)) & 0xffffu);
-                            at[u] = b == 0 ? 0 : static_cast<int>((wa >> (((b - 1) & 1u) * 16)) & 0xffffu);
-                            live[u] = at[u] < end[u];
-                        }
+                        const bool ok = r[u] >= 0 && in_piece(h[u]);
+                        const uint32_t b = bucket_of(h[u]);
+                        const int e_hi = e16[b];
+                        const int e_lo = e16[(b - 1u) & nb_mask];
+                        end[u] = ok ? e_hi : 0;
+                        at[u] = (ok && b != 0u) ? e_lo : 0;
                     }
                     for (;;) {
-                        bool any = false;
+                        bool more = false;
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
-                            if (live[u]) {
-                                uint32_t elo;
-                                const uint32_t e = ExactEntry<K>::get(table, at[u], elo);
-                                ++at[u];
-                                if ((e >> a.row_bits) == fq[u] && elo == ExactEntry<K>::key_lo(k[u])) {
-                                    emit[u] = true;
-                                    brow[u] = e & x_rmask;
-                                    live[u] = false;
-                                } else {
-                                    live[u] = at[u] < end[u];
-                                }
-                            }
-                            any |= live[u];
+                            const bool act = at[u] < end[u];
+                            uint32_t elo;
+                            const uint32_t e = ExactEntry<K>::get(table, act ? at[u] : 0, elo);
+                            const bool hit = act && (e >> a.row_bits) == fq[u] && elo == ExactEntry<K>::key_lo(k[u]);
+                            brow[u] = hit ? (e & x_rmask) : brow[u];
+                            emit[u] = emit[u] || hit;
+                            at[u] = hit ? end[u] : at[u] + (act ? 1 : 0);
+                            more = more || at[u] < end[u];
                         }
-                        if (!any) break;
+                        if (!__any_sync(0xffffffffu, more)) break;
                     }
                     int c = 0;
 #pragma unroll
@@ -964,46 +974,38 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             }
                     });
                 } else if constexpr (UNIQUE && TABLE == TABLE_BUCKET) {
-                    // every tuple matches at most once.  The U tuples walk their
-                    // buckets in lockstep so their shared loads overlap.
-                    bool emit[U], live[U];
+                    // every tuple matches at most once: the predicated walk of
+                    // the EXACT case over {key, row} entries
+                    bool emit[U];
                     uint32_t brow[U];
                     int at[U], end[U];
+                    const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
                         emit[u] = false;
                         brow[u] = 0;
-                        live[u] = r[u] >= 0 && in_piece(h[u]);
-                        at[u] = end[u] = 0;
-                        if (live[u]) {
-                            const uint32_t b = bucket_of(h[u]);
-                            const uint32_t wb = ends[b >> 1];
-                            const uint32_t wa = b == 0 ? 0u : ends[(b - 1) >> 1];
-                            end[u] = static_cast<int>((wb >> ((b & 1u) * 16)) & 0xffffu);
-                            at[u] = b == 0 ? 0 : static_cast<int>((wa >> (((b - 1) & 1u) * 16)) & 0xffffu);
-                            live[u] = at[u] < end[u];
-                        }
+                        const bool ok = r[u] >= 0 && in_piece(h[u]);
+                        const uint32_t b = bucket_of(h[u]);
+                        const int e_hi = e16[b];
+                        const int e_lo = e16[(b - 1u) & nb_mask];
+                        end[u] = ok ? e_hi : 0;
+                        at[u] = (ok && b != 0u) ? e_lo : 0;
                     }
                     for (;;) {
-                        bool any = false;
+                        bool more = false;
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
-                            if (live[u]) {
-                                Cmp ek;
-                                uint32_t er;
-                                E::get(table, at[u], ek, er);
-                                ++at[u];
-                                if (ek == k[u]) {
-                                    emit[u] = true;
-                                    brow[u] = er;
-                                    live[u] = false;
-                                } else {
-                                    live[u] = at[u] < end[u];
-                                }
-                            }
-                            any |= live[u];
+                            const bool act = at[u] < end[u];
+                            Cmp ek;
+                            uint32_t er;
+                            E::get(table, act ? at[u] : 0, ek, er);
+                            const bool hit = act && ek == k[u];
+                            brow[u] = hit ? er : brow[u];
+                            emit[u] = emit[u] || hit;
+                            at[u] = hit ? end[u] : at[u] + (act ? 1 : 0);
+                            more = more || at[u] < end[u];
                         }
-                        if (!any) break;
+                        if (!__any_sync(0xffffffffu, more)) break;
                     }
                     int c = 0;
 #pragma unroll
