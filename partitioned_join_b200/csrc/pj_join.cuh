@@ -458,16 +458,23 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         }
     };
     JobOut jout{};  // batches: the current item's join
-    // Whole warp: every lane appends its c entries; put(stage_index) writes
-    // them into the warp's staging buffer.
+    // The output chunk this warp wrote last and its base: most appends fall
+    // into it again, and then need no look-up of the chunk's base.
+    uint32_t w_ch = 0xffffffffu;
+    long long w_base = 0;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    // Whole warp: every lane appends its c (0..7) entries; put(stage_index)
+    // writes them into the warp's staging buffer.  The positions are the
+    // exclusive prefix of c over the warp, from three bit-sliced ballots.
     auto append = [&](int c, auto&& put) {
-        int incl = c;
+        int excl = 0, n = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+        for (int bit = 0; bit < 3; ++bit) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, (c >> bit) & 1);
+            excl += __popc(bal & lanes_below) << bit;
+            n += __popc(bal) << bit;
         }
-        const int n = __shfl_sync(0xffffffffu, incl, 31);
+        const int incl = excl + c;
         if (n == 0) return;
         if constexpr (BATCH) {
             // exact positions in the join's own output: one atomic per warp step
@@ -497,10 +504,18 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         __syncwarp();
         const uint32_t ch0 = q0 / OUT_CHUNK, ch1 = (q0 + n - 1) / OUT_CHUNK;
         long long b0 = 0, b1 = 0;
-        if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
-        if (lane == 1 && ch1 != ch0) b1 = chunk_base(ch1, true);  // its first position is ours
-        b0 = __shfl_sync(0xffffffffu, b0, 0);
-        b1 = __shfl_sync(0xffffffffu, b1, 1);
+        if (ch0 == w_ch) {
+            b0 = w_base;  // (a chunk's first position, which reserves it, is never a cached chunk)
+        } else {
+            if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
+            b0 = __shfl_sync(0xffffffffu, b0, 0);
+        }
+        if (ch1 != ch0) {
+            if (lane == 1) b1 = chunk_base(ch1, true);  // its first position is ours
+            b1 = __shfl_sync(0xffffffffu, b1, 1);
+        }
+        w_ch = ch1 != ch0 ? (b1 >= 0 ? ch1 : 0xffffffffu) : (b0 >= 0 ? ch0 : 0xffffffffu);
+        w_base = ch1 != ch0 ? b1 : b0;
         // entries [0, n0) go to chunk ch0, the rest to ch1
         const int n0 = ch1 == ch0 ? n : static_cast<int>(ch1 * OUT_CHUNK - q0);
         const uint32_t off0 = q0 % OUT_CHUNK;
@@ -950,6 +965,9 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         bool more = false;
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
+                            // finished cursors read entry 0: a broadcast, no bank
+                            // conflict (reading their own position measured 1.36 ->
+                            // 1.73 ms at 2^27 x 2^27)
                             const bool act = at[u] < end[u];
                             uint32_t elo;
                             const uint32_t e = ExactEntry<K>::get(table, act ? at[u] : 0, elo);
