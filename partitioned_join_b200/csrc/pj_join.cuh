@@ -278,6 +278,28 @@ template <> struct ExactEntry<int64_t> {
     __device__ __forceinline__ static uint32_t key_lo(unsigned long long k) { return static_cast<uint32_t>(k); }
 };
 
+// Shared-memory word load that lanes with pred == false skip: they take no
+// part in the access, so they add no wavefront and no bank conflict.
+__device__ __forceinline__ uint32_t lds_if(const uint32_t* p, bool pred)
+{
+    uint32_t v = 0u;
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q ld.shared.u32 %0, [%1];\n\t}"
+                 : "+r"(v)
+                 : "r"(a), "r"(static_cast<uint32_t>(pred)));
+    return v;
+}
+
+__device__ __forceinline__ uint2 lds2_if(const uint2* p, bool pred)
+{
+    uint2 v = make_uint2(0u, 0u);
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t@q ld.shared.v2.u32 {%0, %1}, [%2];\n\t}"
+                 : "+r"(v.x), "+r"(v.y)
+                 : "r"(a), "r"(static_cast<uint32_t>(pred)));
+    return v;
+}
+
 // Entry of a BUCKET table.
 template <typename K> struct Entry;
 template <> struct Entry<int32_t> {
@@ -458,23 +480,16 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         }
     };
     JobOut jout{};  // batches: the current item's join
-    // The output chunk this warp wrote last and its base: most appends fall
-    // into it again, and then need no look-up of the chunk's base.
-    uint32_t w_ch = 0xffffffffu;
-    long long w_base = 0;
-    const uint32_t lanes_below = (1u << lane) - 1u;
-    // Whole warp: every lane appends its c (0..7) entries; put(stage_index)
-    // writes them into the warp's staging buffer.  The positions are the
-    // exclusive prefix of c over the warp, from three bit-sliced ballots.
+    // Whole warp: every lane appends its c entries; put(stage_index) writes
+    // them into the warp's staging buffer.
     auto append = [&](int c, auto&& put) {
-        int excl = 0, n = 0;
+        int incl = c;
 #pragma unroll
-        for (int bit = 0; bit < 3; ++bit) {
-            const uint32_t bal = __ballot_sync(0xffffffffu, (c >> bit) & 1);
-            excl += __popc(bal & lanes_below) << bit;
-            n += __popc(bal) << bit;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        const int incl = excl + c;
+        const int n = __shfl_sync(0xffffffffu, incl, 31);
         if (n == 0) return;
         if constexpr (BATCH) {
             // exact positions in the join's own output: one atomic per warp step
@@ -504,18 +519,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         __syncwarp();
         const uint32_t ch0 = q0 / OUT_CHUNK, ch1 = (q0 + n - 1) / OUT_CHUNK;
         long long b0 = 0, b1 = 0;
-        if (ch0 == w_ch) {
-            b0 = w_base;  // (a chunk's first position, which reserves it, is never a cached chunk)
-        } else {
-            if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
-            b0 = __shfl_sync(0xffffffffu, b0, 0);
-        }
-        if (ch1 != ch0) {
-            if (lane == 1) b1 = chunk_base(ch1, true);  // its first position is ours
-            b1 = __shfl_sync(0xffffffffu, b1, 1);
-        }
-        w_ch = ch1 != ch0 ? (b1 >= 0 ? ch1 : 0xffffffffu) : (b0 >= 0 ? ch0 : 0xffffffffu);
-        w_base = ch1 != ch0 ? b1 : b0;
+        if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
+        if (lane == 1 && ch1 != ch0) b1 = chunk_base(ch1, true);  // its first position is ours
+        b0 = __shfl_sync(0xffffffffu, b0, 0);
+        b1 = __shfl_sync(0xffffffffu, b1, 1);
         // entries [0, n0) go to chunk ch0, the rest to ch1
         const int n0 = ch1 == ch0 ? n : static_cast<int>(ch1 * OUT_CHUNK - q0);
         const uint32_t off0 = q0 % OUT_CHUNK;
@@ -965,12 +972,19 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         bool more = false;
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
-                            // finished cursors read entry 0: a broadcast, no bank
-                            // conflict (reading their own position measured 1.36 ->
-                            // 1.73 ms at 2^27 x 2^27)
+                            // finished cursors skip the load (4-byte entries) or read
+                            // entry 0, a broadcast: no extra bank conflicts (reading
+                            // their own position measured 1.36 -> 1.73 ms, skipping it
+                            // 1.36 -> 1.31 ms at 2^27 x 2^27)
                             const bool act = at[u] < end[u];
-                            uint32_t elo;
-                            const uint32_t e = ExactEntry<K>::get(table, act ? at[u] : 0, elo);
+                            uint32_t elo = 0u, e;
+                            if constexpr (ExactEntry<K>::BYTES == 4) {
+                                e = lds_if(reinterpret_cast<const uint32_t*>(table) + (act ? at[u] : 0), act);
+                            } else {
+                                const uint2 v = lds2_if(reinterpret_cast<const uint2*>(table) + (act ? at[u] : 0), act);
+                                elo = v.x;
+                                e = v.y;
+                            }
                             const bool hit = act && (e >> a.row_bits) == fq[u] && elo == ExactEntry<K>::key_lo(k[u]);
                             brow[u] = hit ? (e & x_rmask) : brow[u];
                             emit[u] = emit[u] || hit;
@@ -1016,7 +1030,13 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             const bool act = at[u] < end[u];
                             Cmp ek;
                             uint32_t er;
-                            E::get(table, act ? at[u] : 0, ek, er);
+                            if constexpr (Entry<K>::BYTES == 8) {  // skipped by finished cursors
+                                const uint2 v = lds2_if(reinterpret_cast<const uint2*>(table) + (act ? at[u] : 0), act);
+                                ek = v.x;
+                                er = v.y;
+                            } else {
+                                E::get(table, act ? at[u] : 0, ek, er);
+                            }
                             const bool hit = act && ek == k[u];
                             brow[u] = hit ? er : brow[u];
                             emit[u] = emit[u] || hit;
