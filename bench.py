@@ -62,6 +62,8 @@ def parse_args():
                     help="build and probe rows of the bounded CPU sample (log2)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="cfg2: skip the cfg3/cfg4/cfg5 measurements added to the line (other_configs)")
     ap.add_argument("--no-ref-gpu", action="store_true", help="--impl reference: skip the reference's GPU path")
     ap.add_argument("--plan", type=str, default="", help="JSON overrides of pj_plan fields")
     ap.add_argument("--seed", type=int, default=2)
@@ -308,7 +310,7 @@ def reference_gpu(args):
             "timer": "the reference's own stage events (main.cu:769-896), median of 3 runs after 1 warm-up"}
 
 
-def run_ours(args, rank, world, local):
+def run_ours(args, rank, world, local, emit=True):
     import torch
     import torch.distributed as dist
 
@@ -316,7 +318,7 @@ def run_ours(args, rank, world, local):
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    if world > 1:
+    if world > 1 and emit:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
 
@@ -435,10 +437,55 @@ def run_ours(args, rank, world, local):
         line["e2e"] = e2e_measure(args, j, build, probe, stream)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args)
-    if rank == 0:
+    if args.workload == "cfg2" and world == 1 and not args.no_extra:
+        del j, build, probe
+        torch.cuda.empty_cache()
+        line["other_configs"] = other_configs(args, local)
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if world > 1 and emit:
         dist.destroy_process_group()
+    return line
+
+
+def other_configs(args, local):
+    """The other configurations, measured in the same run after the
+    headline (outside its timed region) so that one bench line records
+    them: cfg3 (2^26 x 2^28 int64, Zipf 0 and 1.5), cfg5 (the 512-join
+    batch against the same joins one after another with default and with
+    per-join autotuned plans) and a short cfg4 sweep (16 held-out joins of
+    2^18..2^26 build rows, learned against exact plans)."""
+    import argparse as _ap
+    import torch
+
+    out = {}
+    for zipf in (0.0, 1.5):
+        a = _ap.Namespace(**vars(args))
+        a.workload, a.log2_build, a.log2_probe, a.zipf = "cfg3", 26, 28, zipf
+        a.steps, a.warmup, a.no_e2e, a.no_cpu, a.no_extra, a.plan = min(args.steps, 10), max(args.warmup, 3), True, True, True, ""
+        ln = run_ours(a, 0, 1, local, emit=False)
+        out[f"cfg3_zipf{zipf}"] = {"value": ln["value"], "unit": UNIT, "ms_per_step": ln["ms_per_step"],
+                                   "ms_per_step_median": ln["ms_per_step_median"], "stages_ms": ln["stages_ms"],
+                                   "plan": {k: ln["plan"][k] for k in ("passes", "bits1", "digit_mode", "table_mode",
+                                                                         "n_heavy")},
+                                   "roofline_join_frac": ln["roofline_join"]["frac"],
+                                   "verified": ln["verified"]["last_timed_join"]["ok"] and
+                                   ln["verified"]["warmup_join"]["ok"]}
+        torch.cuda.empty_cache()
+    a = _ap.Namespace(**vars(args))
+    a.workload, a.steps, a.warmup = "cfg5", 5, 3
+    ln = run_batch(a, 0, 1, local, emit=False)
+    out["cfg5"] = {"value": ln["value"], "unit": UNIT, "makespan_ms": ln["makespan_ms"],
+                   "speedup_vs_plain": ln["speedup_vs_plain"], "speedup_vs_plain_autotuned": ln["speedup_vs_plain_autotuned"],
+                   "joins_by_path": ln["joins_by_path"],
+                   "verified": all(v["ok"] for v in ln["verified"].values())}
+    torch.cuda.empty_cache()
+    a = _ap.Namespace(**vars(args))
+    a.workload, a.sweep, a.cfg4_max_log2_build, a.cfg4_max_log2_probe = "cfg4", 16, 26, 27
+    ln = run_learned(a, 0, 1, local, emit=False)
+    out["cfg4_short"] = {"value": ln["value"], "unit": "x", "workload": ln["config"]["workload"],
+                         "fallback_rate": ln["fallback_rate"], "join_ms_total": ln["join_ms_total"]}
+    return out
 
 
 def e2e_measure(args, j, build, probe, stream):
@@ -542,7 +589,7 @@ def cpu_baseline(args):
                       f"inner_join_cpu's own timer (build + probe)"}
 
 
-def run_batch(args, rank, world, local):
+def run_batch(args, rank, world, local, emit=True):
     """cfg5: a batch of int32 joins, build sizes log-uniform in 2^10..2^20
     (unique keys), probe sizes 4x, 70 % uniform matches, every fourth join
     with Zipf(1.0) probe keys -- run one after another with the plain
@@ -688,11 +735,12 @@ def run_batch(args, rank, world, local):
                           if bj.config.large_batched else 0},
         "verified": {"plain": plain_ok, "plain_autotuned": plain_tuned_ok, "batch": batch_ok, "graph": graph_ok},
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
-def run_learned(args, rank, world, local):
+def run_learned(args, rank, world, local, emit=True):
     """cfg4: the shipped planner weights against the exact-histogram planner
     on a held-out seeded sweep (build 2^18..2^28 log-uniform, probe/build 1,
     4 or 16 with the probe side capped at 2^29 rows, int32 or int64, Zipf
@@ -766,8 +814,9 @@ def run_learned(args, rank, world, local):
         "planning_ms_median": {"exact": float(np.median([r["plan_exact_ms"] for r in rows])),
                                "learned": float(np.median([r["plan_learned_ms"] for r in rows]))},
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
