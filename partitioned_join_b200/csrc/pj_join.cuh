@@ -529,16 +529,21 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         if (b0 >= 0 && b0 + off0 + n0 <= a.capacity) {
             int32_t* ob = a.out_build + b0 + off0;
             int32_t* op = a.out_probe + b0 + off0;
-            for (int i = lane; i < n0; i += 32) {
-                st_stream(ob + i, stage_b[i], stream_pol);
-                st_stream(op + i, stage_p[i], stream_pol);
+#pragma unroll
+            for (int t = 0; t < U; ++t) {  // n0 <= 32 * U
+                const int i = lane + 32 * t;
+                if (i < n0) {
+                    st_stream(ob + i, stage_b[i], stream_pol);
+                    st_stream(op + i, stage_p[i], stream_pol);
+                }
             }
         } else {
             for (int i = lane; i < n0; i += 32)
                 if (b0 >= 0) store_out(b0 + off0 + i, stage_b[i], stage_p[i]);
         }
-        for (int i = n0 + lane; i < n; i += 32)
-            if (b1 >= 0) store_out(b1 + (i - n0), stage_b[i], stage_p[i]);
+        if (n0 < n)
+            for (int i = n0 + lane; i < n; i += 32)
+                if (b1 >= 0) store_out(b1 + (i - n0), stage_b[i], stage_p[i]);
         __syncwarp();
     };
 
@@ -638,17 +643,20 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                 uint32_t nh[JOIN_BU];
                 Cmp nk[JOIN_BU];
                 int32_t nr[JOIN_BU];
-                auto load_batch = [&](int64_t i0) {
+                // 32-bit offsets in the item's build range
+                const uint32_t* bt = a.build_tuples + b_lo * TV::WORDS;
+                const uint32_t bn = static_cast<uint32_t>(b_hi - b_lo);
+                auto load_batch = [&](uint32_t i0) {
 #pragma unroll
                     for (int u = 0; u < JOIN_BU; ++u) {
-                        const int64_t i = i0 + u * THREADS;
+                        const uint32_t i = i0 + u * THREADS;
                         nr[u] = -1;
-                        if (i < b_hi) TV::load(a.build_tuples, i, nh[u], nk[u], nr[u]);
+                        if (i < bn) TV::load(bt, i, nh[u], nk[u], nr[u]);
                     }
                 };
-                int64_t i0 = b_lo + threadIdx.x;
-                if (i0 < b_hi) load_batch(i0);
-                for (; i0 < b_hi; i0 += THREADS * JOIN_BU) {
+                uint32_t i0 = threadIdx.x;
+                if (i0 < bn) load_batch(i0);
+                for (; i0 < bn; i0 += THREADS * JOIN_BU) {
                     uint32_t h[JOIN_BU];
                     int32_t r[JOIN_BU];
 #pragma unroll
@@ -656,7 +664,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         h[u] = nh[u];
                         r[u] = nr[u];
                     }
-                    if (i0 + THREADS * JOIN_BU < b_hi) load_batch(i0 + THREADS * JOIN_BU);
+                    if (i0 + THREADS * JOIN_BU < bn) load_batch(i0 + THREADS * JOIN_BU);
 #pragma unroll
                     for (int u = 0; u < JOIN_BU; ++u) {
                         if (r[u] >= 0 && in_piece(h[u])) {
@@ -676,15 +684,17 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             } else {
                 scan_u16_pairs<THREADS>(ends, NB / 2, s_warp);
                 // pass 2: place
-                for (int64_t i0 = b_lo + threadIdx.x; i0 < b_hi; i0 += THREADS * JOIN_BU) {
+                const uint32_t* bt = a.build_tuples + b_lo * TV::WORDS;
+                const uint32_t bn = static_cast<uint32_t>(b_hi - b_lo);
+                for (uint32_t i0 = threadIdx.x; i0 < bn; i0 += THREADS * JOIN_BU) {
                     uint32_t h[JOIN_BU];
                     Cmp k[JOIN_BU];
                     int32_t r[JOIN_BU];
 #pragma unroll
                     for (int u = 0; u < JOIN_BU; ++u) {
-                        const int64_t i = i0 + u * THREADS;
+                        const uint32_t i = i0 + u * THREADS;
                         r[u] = -1;
-                        if (i < b_hi) TV::load(a.build_tuples, i, h[u], k[u], r[u]);
+                        if (i < bn) TV::load(bt, i, h[u], k[u], r[u]);
                     }
 #pragma unroll
                     for (int u = 0; u < JOIN_BU; ++u) {
@@ -693,7 +703,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             const uint32_t old = atomicAdd(&ends[b >> 1], (b & 1u) ? 0x10000u : 1u);
                             const int pos = static_cast<int>((b & 1u) ? (old >> 16) : (old & 0xffffu));
                             if constexpr (TABLE == TABLE_COMPACT)
-                                ctab[pos] = (finger_of(h[u]) << 16) | static_cast<uint32_t>(i0 + u * THREADS - b_lo);
+                                ctab[pos] = (finger_of(h[u]) << 16) | (i0 + u * THREADS);
                             else if constexpr (TABLE == TABLE_EXACT)
                                 ExactEntry<K>::put(table, pos, (xfinger_of(h[u]) << a.row_bits) | static_cast<uint32_t>(r[u]),
                                                    ExactEntry<K>::key_lo(k[u]));
