@@ -777,12 +777,17 @@ def run_learned(args, rank, world, local, emit=True):
 
     for i in range(args.sweep):
         b, p, meta = planner.sweep_workload(rng, args.cfg4_max_log2_build, args.cfg4_max_log2_probe)
+        # planning times on a workspace allocated beforehand (the planners
+        # themselves allocate nothing; the allocation is the caller's)
+        pws = api.alloc_workspace(api.workspace_size(api.make_desc(b, p, True)), b.device)
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        exact = api.plan_exact(b, p, True)
+        exact = api.plan_exact(b, p, True, ws=pws)
         plan_exact_ms = 1e3 * (time.perf_counter() - t0)
         t0 = time.perf_counter()
-        learned, _ = planner.plan_learned(b, p, True, params)
+        learned, _ = planner.plan_learned(b, p, True, params, ws=pws)
         plan_learned_ms = 1e3 * (time.perf_counter() - t0)
+        del pws
         t_exact, st = time_join(b, p, exact)
         _lib.check(st, "exact plan")
         t_learned, st = time_join(b, p, learned)

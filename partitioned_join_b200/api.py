@@ -393,11 +393,15 @@ def join_count(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_
     return int(cnt.item())
 
 
-def plan_exact(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_keys: bool = True) -> Plan:
+def plan_exact(build_keys: torch.Tensor, probe_keys: torch.Tensor, unique_build_keys: bool = True,
+               ws: Optional[torch.Tensor] = None) -> Plan:
+    """The exact-histogram plan (pj_plan_exact).  ws: a workspace of at
+    least the default plan's size to reuse (else one is allocated)."""
     d = make_desc(build_keys, probe_keys, unique_build_keys)
     base = plan_default(d.n_build, d.n_probe, d.key_bytes, unique_build_keys)
     nb = workspace_size(d, base)
-    ws = alloc_workspace(nb, build_keys.device)
+    if ws is None or ws.numel() < nb:
+        ws = alloc_workspace(nb, build_keys.device)
     p = Plan()
     check(lib().pj_plan_exact(ctypes.byref(d), ctypes.c_void_p(ws.data_ptr()), nb, ctypes.byref(p),
                               _stream_ptr(None)), "pj_plan_exact")

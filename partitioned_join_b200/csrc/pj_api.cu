@@ -1723,7 +1723,7 @@ pj_status large_batch_layout(const pj_join_desc* descs, const std::vector<int>& 
         if (!valid_desc(&d) || d.key_bytes != lb.key_bytes) return PJ_ERR_INVALID;
         if (d.n_build == 0 || d.n_probe == 0) continue;  // nothing to join: the count stays 0
         const int bits = std::max(0, bits_for_table(d.n_build, lb.table_cap) + bits_delta);
-        if (bits > LARGE_BATCH_MAX_BITS) continue;  // (scalar key loads: no alignment needed)
+        if (bits > LARGE_BATCH_MAX_BITS) continue;  // run alone (the segment kernels load keys one by one: any alignment)
         take.push_back({i, bits});
         lb.unique = lb.unique && d.unique_build_keys != 0;
         probe_total += d.n_probe;
@@ -1737,6 +1737,9 @@ pj_status large_batch_layout(const pj_join_desc* descs, const std::vector<int>& 
         const int64_t per = (probe_total + static_cast<int64_t>(sm_count()) * 8 - 1) / (static_cast<int64_t>(sm_count()) * 8);
         lb.probe_chunk = static_cast<int32_t>(std::min<int64_t>(std::max<int64_t>(1 << 14, (per + 15) / 16 * 16), 1 << 30));
     }
+    // partitions over all joins: build totals go to [0, G), probe totals to [G, 2G)
+    lb.G = 0;
+    for (const J& j : take) lb.G += 1 << j.bits;
     int64_t cnt = 0, tup = 0, max_items = 0;
     int g = 0;
     for (const J& j : take) {
@@ -1759,7 +1762,7 @@ pj_status large_batch_layout(const pj_join_desc* descs, const std::vector<int>& 
                 it.cnt_base = cnt;
                 it.seg_items = items;
                 it.item = i;
-                it.tot_base = 0;  // set below, once G is known
+                it.tot_base = side == 0 ? g : lb.G + g;
                 it.P = P;
                 it.f = f;
                 lb.seg.push_back(it);
@@ -1786,22 +1789,6 @@ pj_status large_batch_layout(const pj_join_desc* descs, const std::vector<int>& 
         max_items += std::min<int64_t>(max_pieces * max_chunks, static_cast<int64_t>(P) * 4096 + max_pieces + max_chunks);
         lb.joins.push_back(j.idx);
         g += P;
-    }
-    lb.G = g;
-    // tot_base: build totals at [0, G), probe totals at [G, 2G)
-    {
-        size_t at = 0;
-        int gb = 0;
-        for (const J& j : take) {
-            const pj_join_desc& d = descs[j.idx];
-            const int P = 1 << j.bits;
-            for (int side = 0; side < 2; ++side) {
-                const int64_t n = side == 0 ? d.n_build : d.n_probe;
-                const int items = static_cast<int>(std::max<int64_t>(1, (n + SEG_CHUNK - 1) / SEG_CHUNK));
-                for (int i = 0; i < items; ++i) lb.seg[at++].tot_base = side == 0 ? gb : lb.G + gb;
-            }
-            gb += P;
-        }
     }
     lb.n_counts = cnt;
     lb.tuples = tup + 64;

@@ -141,8 +141,10 @@ def candidate(build, probe, c: int, heavy: Plan, unique=True) -> Optional[Plan]:
     return p if st == _lib.OK else None
 
 
-def plan_learned(build, probe, unique=True, params: Optional[torch.Tensor] = None):
-    """(plan, scores) from the network (default: the shipped weights)."""
+def plan_learned(build, probe, unique=True, params: Optional[torch.Tensor] = None,
+                 ws: Optional[torch.Tensor] = None):
+    """(plan, scores) from the network (default: the shipped weights).  ws:
+    a workspace of at least the default plan's size to reuse."""
     if params is None:
         params = load_weights(device=build.device)
         if params is None:
@@ -150,7 +152,8 @@ def plan_learned(build, probe, unique=True, params: Optional[torch.Tensor] = Non
     d = api.make_desc(build, probe, unique)
     base = api.plan_default(d.n_build, d.n_probe, d.key_bytes, unique)
     nb = api.workspace_size(d, base)
-    ws = api.alloc_workspace(nb, build.device)
+    if ws is None or ws.numel() < nb:
+        ws = api.alloc_workspace(nb, build.device)
     p = Plan()
     scores = (ctypes.c_float * _lib.PLAN_CANDIDATES)()
     check(lib().pj_plan_learned(ctypes.byref(d), _p(params), _p(ws), nb, ctypes.byref(p), scores, _st()),
