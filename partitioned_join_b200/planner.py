@@ -298,17 +298,31 @@ def main():
     ap.add_argument("--max-log2-probe", type=int, default=29)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--data", default="", help="save the sweep (npz) here")
+    ap.add_argument("--from-data", default="",
+                    help="train on saved sweeps (comma-separated npz files from --data) instead of sweeping")
     a = ap.parse_args()
     rng = np.random.default_rng(a.seed)
     F, T, FAIL, TEX, META = [], [], [], [], []
     t0 = time.time()
-    for i in range(a.workloads):
+    if a.from_data:
+        for path in a.from_data.split(","):
+            z = np.load(path)
+            F += list(z["features"])
+            T += list(z["times"])
+            FAIL += list(z["failed"])
+            TEX += list(z["t_exact"])
+            META += json.loads(str(z["meta"]))
+        # shuffle with the seed so that the held-out split mixes the sweeps
+        order = rng.permutation(len(F))
+        F, T, FAIL, TEX, META = ([x[i] for i in order] for x in (F, T, FAIL, TEX, META))
+        a.workloads = len(F)
+    for i in range(0 if a.from_data else a.workloads):
         b, p, meta = sweep_workload(rng, a.max_log2_build, a.max_log2_probe, min_log2_build=a.min_log2_build)
         f, t, fl, te = measure(b, p)
         F.append(f), T.append(t), FAIL.append(fl), TEX.append(te), META.append(meta)
         del b, p
     F, T, FAIL, TEX = (np.array(x) for x in (F, T, FAIL, TEX))
-    if a.data:
+    if a.data and not a.from_data:
         np.savez(a.data, features=F, times=T, failed=FAIL, t_exact=TEX, meta=json.dumps(META))
     tgt, mask = targets(T, FAIL, TEX)
     n_test = int(round(a.held_out * len(F)))
@@ -319,7 +333,8 @@ def main():
               "held_out": evaluate(net.predict(F[te]), T[te], FAIL[te], TEX[te]),
               "loss_first_last": [losses[0], losses[-1]], "sweep_seconds": time.time() - t0,
               "sweep": {"workloads": a.workloads, "seed": a.seed, "min_log2_build": a.min_log2_build,
-                        "max_log2_build": a.max_log2_build, "max_log2_probe": a.max_log2_probe},
+                        "max_log2_build": a.max_log2_build, "max_log2_probe": a.max_log2_probe,
+                        "from_data": a.from_data},
         "candidates": _lib.PLAN_CANDIDATES}
     np.savez(a.out, params=net.params.cpu().numpy(), report=json.dumps(report))
     print(json.dumps(report))
