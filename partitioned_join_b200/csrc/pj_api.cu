@@ -6,7 +6,6 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
-#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -290,12 +289,28 @@ int bits_for_table(int64_t n_build, int64_t cap)
 // the share of the sample they cover.
 double heavy_from_sample(const std::vector<int64_t>& keys, int min_count, pj_plan* plan)
 {
-    std::unordered_map<int64_t, int> freq;
-    freq.reserve(keys.size());
-    for (int64_t k : keys) ++freq[k];
+    // Key frequencies in an open-addressing table (linear probing, at most
+    // half full): a planning call counts up to 65 536 sampled keys, and a
+    // node-based hash map took milliseconds for that.
+    size_t cap = 16;
+    while (cap < 2 * keys.size()) cap <<= 1;
+    std::vector<int64_t> slot_key(cap);
+    std::vector<int32_t> slot_count(cap, 0);  // 0: empty
+    for (int64_t k : keys) {
+        uint64_t x = static_cast<uint64_t>(k);  // splitmix64 finaliser as the table's hash
+        x ^= x >> 30;
+        x *= 0xbf58476d1ce4e5b9ull;
+        x ^= x >> 27;
+        x *= 0x94d049bb133111ebull;
+        x ^= x >> 31;
+        size_t i = static_cast<size_t>(x) & (cap - 1);
+        while (slot_count[i] != 0 && slot_key[i] != k) i = (i + 1) & (cap - 1);
+        slot_key[i] = k;
+        ++slot_count[i];
+    }
     std::vector<std::pair<int, int64_t>> heavy;
-    for (const auto& kv : freq)
-        if (kv.second >= min_count) heavy.emplace_back(kv.second, kv.first);
+    for (size_t i = 0; i < cap; ++i)
+        if (slot_count[i] >= min_count) heavy.emplace_back(slot_count[i], slot_key[i]);
     std::sort(heavy.begin(), heavy.end(), [](const auto& x, const auto& y) {
         return x.first != y.first ? x.first > y.first : x.second < y.second;
     });
