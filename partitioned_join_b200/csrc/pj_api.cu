@@ -144,10 +144,10 @@ template <typename K>
 size_t join_smem_k(int table_mode, int cap, int nb)
 {
     switch (table_mode) {
-    case PJ_TABLE_BUCKET: return JoinSmem<K, TABLE_BUCKET>::bytes(cap, nb, JN_THREADS);
-    case PJ_TABLE_COMPACT: return JoinSmem<K, TABLE_COMPACT>::bytes(cap, nb, JN_THREADS);
-    case PJ_TABLE_EXACT: return JoinSmem<K, TABLE_EXACT>::bytes(cap, nb, JN_THREADS);
-    default: return JoinSmem<K, TABLE_OPEN>::bytes(cap, nb, JN_THREADS);
+    case PJ_TABLE_BUCKET: return JoinSmem<K, TABLE_BUCKET>::bytes(cap, nb);
+    case PJ_TABLE_COMPACT: return JoinSmem<K, TABLE_COMPACT>::bytes(cap, nb);
+    case PJ_TABLE_EXACT: return JoinSmem<K, TABLE_EXACT>::bytes(cap, nb);
+    default: return JoinSmem<K, TABLE_OPEN>::bytes(cap, nb);
     }
 }
 
@@ -697,7 +697,7 @@ template <typename K, int TABLE, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF>
 pj_status launch_join_t(const JoinArgs& a, cudaStream_t st)
 {
     auto* kern = join_kernel<K, TABLE, UNIQUE, HASH_SPLIT, SLOT_REF, JN_THREADS>;
-    const size_t smem = JoinSmem<K, TABLE>::bytes(a.cap, a.nb_log2, JN_THREADS);
+    const size_t smem = JoinSmem<K, TABLE>::bytes(a.cap, a.nb_log2);
     PJ_CUDA(set_smem(kern, smem));
     int per_sm = 0;
     PJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, JN_THREADS, smem));
@@ -1705,7 +1705,7 @@ pj_status large_batch_run_t(const LargeBatch& lb, void* ws, uint32_t* status, cu
     a.parts = parts;
     a.outs = reinterpret_cast<const JobOut*>(w + lb.o_outs);
     auto launch = [&](auto* kern) -> pj_status {
-        const size_t smem = JoinSmem<K, TABLE_BUCKET>::bytes(a.cap, a.nb_log2, JN_THREADS);
+        const size_t smem = JoinSmem<K, TABLE_BUCKET>::bytes(a.cap, a.nb_log2);
         PJ_CUDA(set_smem(kern, smem));
         int per_sm = 0;
         PJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, JN_THREADS, smem));

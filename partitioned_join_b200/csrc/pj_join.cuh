@@ -31,13 +31,14 @@
 //     a CAS on the row word claims a slot, row == -1 marks it empty, so every
 //     key value (the reference's -1 sentinel included) joins.
 //
-// Output.  Probing has no block-wide barrier: each warp stages its matches
-// in a small shared buffer (ballot/scan compaction), reserves their
-// positions with one shared atomic on the CTA's entry counter and copies
-// them out coalesced.  A CTA claims output space from the global counter
-// OUT_CHUNK entries at a time, so global atomics are rare (the reference's
-// write_back_buffer, hash_join_kernels.cuh:150-199, does one per match past
-// its buffer).  Each CTA's last chunk is only partly used; a fix-up pass
+// Output.  Probing has no block-wide barrier: each warp numbers a step's
+// matches with ballots (all lanes' first tuple's matches, then the second
+// tuple's, ...), reserves their positions with one shared atomic on the
+// CTA's entry counter and stores them straight from registers, each store
+// instruction one contiguous run.  A CTA claims output space from the
+// global counter OUT_CHUNK entries at a time, so global atomics are rare
+// (the reference's write_back_buffer, hash_join_kernels.cuh:150-199, does
+// one per match past its buffer).  Each CTA's last chunk is only partly used; a fix-up pass
 // (join_fixup_plan_kernel / join_fixup_move_kernel) moves the entries above
 // the true total into those gaps, so the output is dense.
 #pragma once
@@ -278,26 +279,71 @@ template <> struct ExactEntry<int64_t> {
     __device__ __forceinline__ static uint32_t key_lo(unsigned long long k) { return static_cast<uint32_t>(k); }
 };
 
-// Shared-memory word load that lanes with pred == false skip: they take no
-// part in the access, so they add no wavefront and no bank conflict.
-__device__ __forceinline__ uint32_t lds_if(const uint32_t* p, bool pred)
+// One pass of the predicated bucket walk for one probe tuple, in PTX so that
+// the cursor test, the skipped load and the updates are all predicated
+// instructions.  at / end: shared-window byte addresses of the tuple's
+// cursor and of its bucket's end; a lane whose cursor has reached the end
+// skips the load (no wavefront, no bank conflict).  On a match raw takes
+// the entry's row word, hit becomes 1 and end = at, so the walk stops.
+//
+// 4-byte EXACT entries: e matches when (e ^ fqs) < lim, i.e. its bits above
+// the row bits equal the tuple's tag (fqs = tag << R, lim = 1 << R).
+__device__ __forceinline__ void walk_exact4(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t fqs,
+                                            uint32_t lim)
 {
-    uint32_t v = 0u;
-    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
-    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q ld.shared.u32 %0, [%1];\n\t}"
-                 : "+r"(v)
-                 : "r"(a), "r"(static_cast<uint32_t>(pred)));
-    return v;
+    asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 e, t;\n\t"
+                 "mov.b32 e, 0;\n\t"
+                 "setp.lt.u32 p, %0, %1;\n\t"
+                 "@p ld.shared.u32 e, [%0];\n\t"
+                 "xor.b32 t, e, %4;\n\t"
+                 "setp.lt.and.u32 q, t, %5, p;\n\t"
+                 "@q mov.b32 %2, e;\n\t"
+                 "@q mov.b32 %1, %0;\n\t"
+                 "@q mov.b32 %3, 1;\n\t"
+                 "@p add.u32 %0, %0, 4;\n\t"
+                 "}"
+                 : "+r"(at), "+r"(end), "+r"(raw), "+r"(hit)
+                 : "r"(fqs), "r"(lim));
 }
 
-__device__ __forceinline__ uint2 lds2_if(const uint2* p, bool pred)
+// 8-byte EXACT entries {key low word, tag << R | row}: the low word must
+// equal the tuple's too.
+__device__ __forceinline__ void walk_exact8(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t fqs,
+                                            uint32_t lim, uint32_t klo)
 {
-    uint2 v = make_uint2(0u, 0u);
-    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
-    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t@q ld.shared.v2.u32 {%0, %1}, [%2];\n\t}"
-                 : "+r"(v.x), "+r"(v.y)
-                 : "r"(a), "r"(static_cast<uint32_t>(pred)));
-    return v;
+    asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 lo, e, t;\n\t"
+                 "mov.b32 lo, 0;\n\t"
+                 "mov.b32 e, 0;\n\t"
+                 "setp.lt.u32 p, %0, %1;\n\t"
+                 "@p ld.shared.v2.u32 {lo, e}, [%0];\n\t"
+                 "xor.b32 t, e, %4;\n\t"
+                 "setp.lt.and.u32 q, t, %5, p;\n\t"
+                 "setp.eq.and.u32 q, lo, %6, q;\n\t"
+                 "@q mov.b32 %2, e;\n\t"
+                 "@q mov.b32 %1, %0;\n\t"
+                 "@q mov.b32 %3, 1;\n\t"
+                 "@p add.u32 %0, %0, 8;\n\t"
+                 "}"
+                 : "+r"(at), "+r"(end), "+r"(raw), "+r"(hit)
+                 : "r"(fqs), "r"(lim), "r"(klo));
+}
+
+// 8-byte BUCKET entries {key, row} of 4-byte keys: a match is key == k.
+__device__ __forceinline__ void walk_bucket8(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t k)
+{
+    asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 ek, er;\n\t"
+                 "mov.b32 ek, 0;\n\t"
+                 "mov.b32 er, 0;\n\t"
+                 "setp.lt.u32 p, %0, %1;\n\t"
+                 "@p ld.shared.v2.u32 {ek, er}, [%0];\n\t"
+                 "setp.eq.and.u32 q, ek, %4, p;\n\t"
+                 "@q mov.b32 %2, er;\n\t"
+                 "@q mov.b32 %1, %0;\n\t"
+                 "@q mov.b32 %3, 1;\n\t"
+                 "@p add.u32 %0, %0, 8;\n\t"
+                 "}"
+                 : "+r"(at), "+r"(end), "+r"(raw), "+r"(hit)
+                 : "r"(k));
 }
 
 // Entry of a BUCKET table.
@@ -367,7 +413,7 @@ constexpr int64_t PROBE_PREFETCH_BYTES = 128 << 10;
 // Output geometry.
 constexpr int OUT_CHUNK = 8192;  // entries a CTA claims per global atomic
 constexpr int OUT_SLOTS = 16;    // chunk bases a CTA keeps in shared memory
-constexpr int JOIN_U = 4;        // probe tuples in flight per lane (and staged entries per lane)
+constexpr int JOIN_U = 4;        // probe tuples in flight per lane
 constexpr int JOIN_BU = 4;       // build tuples in flight per thread
 
 template <typename K, int TABLE>
@@ -387,11 +433,9 @@ struct JoinSmem {
         if (TABLE != TABLE_OPEN) t += ((static_cast<size_t>(1) << nb_log2) / 2) * 4;
         return (t + 127) & ~size_t(127);
     }
-    // plus per-warp staging of 32 * JOIN_U entries (build and probe rows)
-    __host__ __device__ static size_t bytes(int cap, int nb_log2, int threads)
-    {
-        return table_bytes(cap, nb_log2) + static_cast<size_t>(threads / 32) * 32 * JOIN_U * 8;
-    }
+    // dynamic shared memory of a join CTA: the table alone (matches go
+    // straight from registers to global memory)
+    __host__ __device__ static size_t bytes(int cap, int nb_log2) { return table_bytes(cap, nb_log2); }
 };
 
 template <typename K, int TABLE, bool UNIQUE, bool HASH_SPLIT, bool SLOT_REF, int THREADS, bool BATCH = false>
@@ -402,16 +446,12 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     using E = Entry<K>;
     using SM = JoinSmem<K, TABLE>;
     constexpr int NWARPS = THREADS / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    auto warp_id = [&]() { return warp; };
+    const int lane = threadIdx.x & 31;
     constexpr int U = JOIN_U;
 
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* table = smem;
     uint32_t* ends = reinterpret_cast<uint32_t*>(smem + SM::entries_bytes(a.cap));
-    constexpr int STAGE = 32 * U;  // staged entries per warp
-    int32_t* stage_b = reinterpret_cast<int32_t*>(smem + SM::table_bytes(a.cap, a.nb_log2)) + warp_id() * 2 * STAGE;
-    int32_t* stage_p = stage_b + STAGE;
     // OPEN tables of 8-byte keys: keys[cap] (8 B) then rows[cap]
     unsigned long long* okeys = reinterpret_cast<unsigned long long*>(table);
     uint32_t* ctab = reinterpret_cast<uint32_t*>(table);  // COMPACT: fingerprint << 16 | index
@@ -480,16 +520,20 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         }
     };
     JobOut jout{};  // batches: the current item's join
-    // Whole warp: every lane appends its c entries; put(stage_index) writes
-    // them into the warp's staging buffer.
-    auto append = [&](int c, auto&& put) {
-        int incl = c;
+    // Whole warp: lane l appends (brow[u], rp[u]) for every u with emit[u].
+    // The step's entries are laid out u-major (all lanes' u = 0 entries, then
+    // u = 1, ...), so each store instruction writes one contiguous run and
+    // no staging buffer is needed.
+    auto append_direct = [&](const bool (&emit)[U], const uint32_t (&brow)[U], const int32_t (&rp)[U]) {
+        const uint32_t lt = (1u << lane) - 1u;
+        int off[U];
+        int n = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+        for (int u = 0; u < U; ++u) {
+            const uint32_t m = __ballot_sync(0xffffffffu, emit[u]);
+            off[u] = n + __popc(m & lt);
+            n += __popc(m);
         }
-        const int n = __shfl_sync(0xffffffffu, incl, 31);
         if (n == 0) return;
         if constexpr (BATCH) {
             // exact positions in the join's own output: one atomic per warp step
@@ -497,56 +541,53 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             if (lane == 0) q0 = atomicAdd(jout.count, static_cast<unsigned long long>(n));
             q0 = __shfl_sync(0xffffffffu, q0, 0);
             if (jout.out_build == nullptr) return;
-            put(incl - c);
-            __syncwarp();
-            for (int i = lane; i < n; i += 32) {
-                const long long pos = static_cast<long long>(q0) + i;
-                if (pos < jout.capacity) {
-                    st_stream(jout.out_build + pos, stage_b[i], stream_pol);
-                    st_stream(jout.out_probe + pos, stage_p[i], stream_pol);
-                } else {
-                    raise_status(a.status, ST_CAPACITY);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (emit[u]) {
+                    const long long pos = static_cast<long long>(q0) + off[u];
+                    if (pos < jout.capacity) {
+                        st_stream(jout.out_build + pos, static_cast<int32_t>(brow[u]), stream_pol);
+                        st_stream(jout.out_probe + pos, rp[u], stream_pol);
+                    } else {
+                        raise_status(a.status, ST_CAPACITY);
+                    }
                 }
-            }
-            __syncwarp();
             return;
         }
         uint32_t q0 = 0;
         if (lane == 0) q0 = atomicAdd(&s_q, static_cast<uint32_t>(n));
         q0 = __shfl_sync(0xffffffffu, q0, 0);
         if (!write_out) return;  // count only
-        put(incl - c);
-        __syncwarp();
         const uint32_t ch0 = q0 / OUT_CHUNK, ch1 = (q0 + n - 1) / OUT_CHUNK;
         long long b0 = 0, b1 = 0;
         if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
         if (lane == 1 && ch1 != ch0) b1 = chunk_base(ch1, true);  // its first position is ours
         b0 = __shfl_sync(0xffffffffu, b0, 0);
         b1 = __shfl_sync(0xffffffffu, b1, 1);
-        // entries [0, n0) go to chunk ch0, the rest to ch1
+        // entries [0, n0) go to chunk ch0 from position p0, the rest to ch1
         const int n0 = ch1 == ch0 ? n : static_cast<int>(ch1 * OUT_CHUNK - q0);
-        const uint32_t off0 = q0 % OUT_CHUNK;
-        if (b0 >= 0 && b0 + off0 + n0 <= a.capacity) {
-            int32_t* ob = a.out_build + b0 + off0;
-            int32_t* op = a.out_probe + b0 + off0;
+        const long long p0 = b0 + static_cast<long long>(q0 % OUT_CHUNK);
+        const long long p1 = b1 - n0;
+        if (b0 >= 0 && p0 + n0 <= a.capacity && (n0 == n || (b1 >= 0 && b1 + (n - n0) <= a.capacity))) {
 #pragma unroll
-            for (int t = 0; t < U; ++t) {  // n0 <= 32 * U
-                const int i = lane + 32 * t;
-                if (i < n0) {
-                    st_stream(ob + i, stage_b[i], stream_pol);
-                    st_stream(op + i, stage_p[i], stream_pol);
+            for (int u = 0; u < U; ++u)
+                if (emit[u]) {
+                    const long long pos = (off[u] < n0 ? p0 : p1) + off[u];
+                    st_stream(a.out_build + pos, static_cast<int32_t>(brow[u]), stream_pol);
+                    st_stream(a.out_probe + pos, rp[u], stream_pol);
                 }
-            }
         } else {
-            for (int i = lane; i < n0; i += 32)
-                if (b0 >= 0) store_out(b0 + off0 + i, stage_b[i], stage_p[i]);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (emit[u]) {
+                    if (off[u] < n0) {
+                        if (b0 >= 0) store_out(p0 + off[u], static_cast<int32_t>(brow[u]), rp[u]);
+                    } else if (b1 >= 0) {
+                        store_out(p1 + off[u], static_cast<int32_t>(brow[u]), rp[u]);
+                    }
+                }
         }
-        if (n0 < n)
-            for (int i = n0 + lane; i < n; i += 32)
-                if (b1 >= 0) store_out(b1 + (i - n0), stage_b[i], stage_p[i]);
-        __syncwarp();
     };
-
     bool first_item = true;
     for (;;) {
         __syncthreads();
@@ -944,134 +985,119 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         }
                         if (!__any_sync(0xffffffffu, again)) break;
                     }
-                    int c = 0;
-#pragma unroll
-                    for (int u = 0; u < U; ++u) c += emit[u] ? 1 : 0;
-                    append(c, [&](int at_stage) {
-#pragma unroll
-                        for (int u = 0; u < U; ++u)
-                            if (emit[u]) {
-                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
-                                stage_p[at_stage] = r[u];
-                                ++at_stage;
-                            }
-                    });
+                    append_direct(emit, brow, r);
                 } else if constexpr (UNIQUE && TABLE == TABLE_EXACT) {
                     // every tuple matches at most once, and an entry's bits decide
                     // it.  Predicated walk: each pass looks at one entry of every
-                    // unfinished tuple, selects instead of branches, and the loop
-                    // runs while any lane has one left (2^27 x 2^27 int32 join
-                    // 1.72 -> 1.53 ms against a branchy lockstep walk)
+                    // unfinished tuple (walk_exact4/8) and the loop runs while any
+                    // lane has one left; finished cursors skip their load.  2^27 x
+                    // 2^27 int32 join: 1.72 ms with a branchy lockstep walk, 1.53
+                    // with selects, 1.31 with skipped loads and build prefetches.
+                    constexpr uint32_t EB = ExactEntry<K>::BYTES;
+                    const uint32_t tb = static_cast<uint32_t>(__cvta_generic_to_shared(table));
+                    const uint32_t lim = 1u << a.row_bits;
                     bool emit[U];
-                    uint32_t brow[U], fq[U];
-                    int at[U], end[U];
+                    uint32_t brow[U], raw[U], hit[U], fqs[U], at[U], end[U];
                     const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        emit[u] = false;
-                        brow[u] = 0;
-                        fq[u] = xfinger_of(h[u]);
+                        raw[u] = 0u;
+                        hit[u] = 0u;
+                        fqs[u] = xfinger_of(h[u]) << a.row_bits;
                         const bool ok = r[u] >= 0 && in_piece(h[u]);
                         const uint32_t b = bucket_of(h[u]);
-                        const int e_hi = e16[b];
-                        const int e_lo = e16[(b - 1u) & nb_mask];
-                        end[u] = ok ? e_hi : 0;
-                        at[u] = (ok && b != 0u) ? e_lo : 0;
+                        const uint32_t e_hi = e16[b];
+                        const uint32_t e_lo = e16[(b - 1u) & nb_mask];
+                        end[u] = tb + (ok ? e_hi : 0u) * EB;
+                        at[u] = tb + ((ok && b != 0u) ? e_lo : 0u) * EB;
                     }
                     for (;;) {
                         bool more = false;
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
-                            // finished cursors skip the load (4-byte entries) or read
-                            // entry 0, a broadcast: no extra bank conflicts (reading
-                            // their own position measured 1.36 -> 1.73 ms, skipping it
-                            // 1.36 -> 1.31 ms at 2^27 x 2^27)
-                            const bool act = at[u] < end[u];
-                            uint32_t elo = 0u, e;
-                            if constexpr (ExactEntry<K>::BYTES == 4) {
-                                e = lds_if(reinterpret_cast<const uint32_t*>(table) + (act ? at[u] : 0), act);
-                            } else {
-                                const uint2 v = lds2_if(reinterpret_cast<const uint2*>(table) + (act ? at[u] : 0), act);
-                                elo = v.x;
-                                e = v.y;
-                            }
-                            const bool hit = act && (e >> a.row_bits) == fq[u] && elo == ExactEntry<K>::key_lo(k[u]);
-                            brow[u] = hit ? (e & x_rmask) : brow[u];
-                            emit[u] = emit[u] || hit;
-                            at[u] = hit ? end[u] : at[u] + (act ? 1 : 0);
+                            if constexpr (EB == 4)
+                                walk_exact4(at[u], end[u], raw[u], hit[u], fqs[u], lim);
+                            else
+                                walk_exact8(at[u], end[u], raw[u], hit[u], fqs[u], lim, ExactEntry<K>::key_lo(k[u]));
                             more = more || at[u] < end[u];
                         }
                         if (!__any_sync(0xffffffffu, more)) break;
                     }
-                    int c = 0;
 #pragma unroll
-                    for (int u = 0; u < U; ++u) c += emit[u] ? 1 : 0;
-                    append(c, [&](int at_stage) {
-#pragma unroll
-                        for (int u = 0; u < U; ++u)
-                            if (emit[u]) {
-                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
-                                stage_p[at_stage] = r[u];
-                                ++at_stage;
-                            }
-                    });
+                    for (int u = 0; u < U; ++u) {
+                        emit[u] = hit[u] != 0u;
+                        brow[u] = raw[u] & x_rmask;
+                    }
+                    append_direct(emit, brow, r);
                 } else if constexpr (UNIQUE && TABLE == TABLE_BUCKET) {
                     // every tuple matches at most once: the predicated walk of
                     // the EXACT case over {key, row} entries
-                    bool emit[U];
-                    uint32_t brow[U];
-                    int at[U], end[U];
-                    const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
-#pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        emit[u] = false;
-                        brow[u] = 0;
-                        const bool ok = r[u] >= 0 && in_piece(h[u]);
-                        const uint32_t b = bucket_of(h[u]);
-                        const int e_hi = e16[b];
-                        const int e_lo = e16[(b - 1u) & nb_mask];
-                        end[u] = ok ? e_hi : 0;
-                        at[u] = (ok && b != 0u) ? e_lo : 0;
-                    }
-                    for (;;) {
-                        bool more = false;
+                    if constexpr (Entry<K>::BYTES == 8) {
+                        const uint32_t tb = static_cast<uint32_t>(__cvta_generic_to_shared(table));
+                        bool emit[U];
+                        uint32_t brow[U], hit[U], at[U], end[U];
+                        const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
-                            const bool act = at[u] < end[u];
-                            Cmp ek;
-                            uint32_t er;
-                            if constexpr (Entry<K>::BYTES == 8) {  // skipped by finished cursors
-                                const uint2 v = lds2_if(reinterpret_cast<const uint2*>(table) + (act ? at[u] : 0), act);
-                                ek = v.x;
-                                er = v.y;
-                            } else {
-                                E::get(table, act ? at[u] : 0, ek, er);
-                            }
-                            const bool hit = act && ek == k[u];
-                            brow[u] = hit ? er : brow[u];
-                            emit[u] = emit[u] || hit;
-                            at[u] = hit ? end[u] : at[u] + (act ? 1 : 0);
-                            more = more || at[u] < end[u];
+                            brow[u] = 0u;
+                            hit[u] = 0u;
+                            const bool ok = r[u] >= 0 && in_piece(h[u]);
+                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t e_hi = e16[b];
+                            const uint32_t e_lo = e16[(b - 1u) & nb_mask];
+                            end[u] = tb + (ok ? e_hi : 0u) * 8u;
+                            at[u] = tb + ((ok && b != 0u) ? e_lo : 0u) * 8u;
                         }
-                        if (!__any_sync(0xffffffffu, more)) break;
-                    }
-                    int c = 0;
+                        for (;;) {
+                            bool more = false;
 #pragma unroll
-                    for (int u = 0; u < U; ++u) c += emit[u] ? 1 : 0;
-                    append(c, [&](int at_stage) {
-#pragma unroll
-                        for (int u = 0; u < U; ++u)
-                            if (emit[u]) {
-                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
-                                stage_p[at_stage] = r[u];
-                                ++at_stage;
+                            for (int u = 0; u < U; ++u) {
+                                walk_bucket8(at[u], end[u], brow[u], hit[u], static_cast<uint32_t>(k[u]));
+                                more = more || at[u] < end[u];
                             }
-                    });
+                            if (!__any_sync(0xffffffffu, more)) break;
+                        }
+#pragma unroll
+                        for (int u = 0; u < U; ++u) emit[u] = hit[u] != 0u;
+                        append_direct(emit, brow, r);
+                    } else {  // 12-byte entries {key, row} of 8-byte keys
+                        bool emit[U];
+                        uint32_t brow[U];
+                        int at[U], end[U];
+                        const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            emit[u] = false;
+                            brow[u] = 0;
+                            const bool ok = r[u] >= 0 && in_piece(h[u]);
+                            const uint32_t b = bucket_of(h[u]);
+                            const int e_hi = e16[b];
+                            const int e_lo = e16[(b - 1u) & nb_mask];
+                            end[u] = ok ? e_hi : 0;
+                            at[u] = (ok && b != 0u) ? e_lo : 0;
+                        }
+                        for (;;) {
+                            bool more = false;
+#pragma unroll
+                            for (int u = 0; u < U; ++u) {
+                                const bool act = at[u] < end[u];
+                                Cmp ek;
+                                uint32_t er;
+                                E::get(table, act ? at[u] : 0, ek, er);
+                                const bool hit = act && ek == k[u];
+                                brow[u] = hit ? er : brow[u];
+                                emit[u] = emit[u] || hit;
+                                at[u] = hit ? end[u] : at[u] + (act ? 1 : 0);
+                                more = more || at[u] < end[u];
+                            }
+                            if (!__any_sync(0xffffffffu, more)) break;
+                        }
+                        append_direct(emit, brow, r);
+                    }
                 } else if constexpr (UNIQUE) {
                     // every tuple matches at most once: one lookup, one append per warp step
                     bool emit[U];
                     uint32_t brow[U];
-                    int c = 0;
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
                         emit[u] = false;
@@ -1083,17 +1109,8 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             start(u, at_u, end_u, sl_u);
                             emit[u] = lookup(u, at_u, end_u, sl_u, steps_u, live_u, brow[u]);
                         }
-                        c += emit[u] ? 1 : 0;
                     }
-                    append(c, [&](int at_stage) {
-#pragma unroll
-                        for (int u = 0; u < U; ++u)
-                            if (emit[u]) {
-                                stage_b[at_stage] = static_cast<int32_t>(brow[u]);
-                                stage_p[at_stage] = r[u];
-                                ++at_stage;
-                            }
-                    });
+                    append_direct(emit, brow, r);
                 } else {
                     // repeated build keys: every tuple walks on, one match per lane per append
                     bool live[U], emit[U];
@@ -1108,23 +1125,13 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         if (live[u]) start(u, at[u], end[u], sl[u]);
                     }
                     for (;;) {
-                        int c = 0;
                         bool any_live = false;
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
                             emit[u] = live[u] && lookup(u, at[u], end[u], sl[u], steps[u], live[u], brow[u]);
-                            c += emit[u] ? 1 : 0;
                             any_live |= live[u];
                         }
-                        append(c, [&](int at_stage) {
-#pragma unroll
-                            for (int u = 0; u < U; ++u)
-                                if (emit[u]) {
-                                    stage_b[at_stage] = static_cast<int32_t>(brow[u]);
-                                    stage_p[at_stage] = r[u];
-                                    ++at_stage;
-                                }
-                        });
+                        append_direct(emit, brow, r);
                         if (!__any_sync(0xffffffffu, any_live)) break;
                     }
                 }
