@@ -416,6 +416,19 @@ constexpr int OUT_SLOTS = 16;    // chunk bases a CTA keeps in shared memory
 constexpr int JOIN_U = 4;        // probe tuples in flight per lane
 constexpr int JOIN_BU = 4;       // build tuples in flight per thread
 
+// Where one work item's tuples are.  Thread 0 works it out for the next
+// item while the current one probes, so an item starts without a chain of
+// dependent global loads (item -> partition -> offsets).
+struct ItemMeta {
+    int64_t b_lo, b_hi;  // build tuples of the item's piece
+    int64_t q_lo, q_hi;  // probe tuples of the item's chunk
+    int32_t p;           // partition
+    int32_t piece;       // build piece (hash split: the piece's hash bits)
+    int32_t sbits;       // hash split bits (0: no hash split)
+    int32_t dbits;       // top hash bits the partition digits consumed
+    JobOut jout;         // batches: the item's join
+};
+
 template <typename K, int TABLE>
 struct JoinSmem {
     // table bytes for capacity cap (BUCKET: tuples; OPEN: slots) and 2^nb_log2 buckets
@@ -463,6 +476,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     __shared__ uint32_t s_warp[NWARPS];
     __shared__ int s_nbuild;
     __shared__ uint32_t s_step;  // next probe step of the current item
+    __shared__ ItemMeta s_cur, s_nxt;  // the current and the next item
 
     const uint64_t stream_pol = l2_evict_first_policy();
     const int NB = 1 << a.nb_log2;
@@ -470,9 +484,49 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
     const int64_t total_items = a.item_off[a.P];
     const bool write_out = a.out_build != nullptr;
 
+    auto load_meta = [&](int64_t it) -> ItemMeta {
+        ItemMeta m;
+        const int p = a.item_part[it];
+        const int64_t local = it - a.item_off[p];
+        const int32_t split = a.split[p];
+        const int64_t S = HASH_SPLIT ? (1ll << split) : split;
+        const int64_t piece = local % S;
+        const int64_t pchunk = local / S;
+        int64_t b_at = static_cast<int64_t>(p) * a.b_items, p_at = static_cast<int64_t>(p) * a.p_items;
+        int32_t b_n = a.b_items, p_n = a.p_items;
+        m.dbits = a.digit_bits;
+        m.jout = JobOut{};
+        if constexpr (BATCH) {
+            const PartRef r = a.parts[p];
+            b_at = r.b_at;
+            p_at = r.p_at;
+            b_n = r.b_items;
+            p_n = r.p_items;
+            m.dbits = r.digit_bits;
+            m.jout = a.outs[r.job];
+        }
+        const int64_t b_lo0 = a.build_off[b_at];
+        const int64_t b_hi0 = a.build_off[b_at + b_n];
+        m.b_lo = b_lo0;
+        m.b_hi = b_hi0;
+        if (!HASH_SPLIT) {
+            m.b_lo = b_lo0 + piece * a.position_chunk;
+            m.b_hi = m.b_lo + a.position_chunk < b_hi0 ? m.b_lo + a.position_chunk : b_hi0;
+            if (m.b_lo > m.b_hi) m.b_lo = m.b_hi;
+        }
+        const int64_t q_lo0 = a.probe_off[p_at];
+        const int64_t q_hi0 = a.probe_off[p_at + p_n];
+        m.q_lo = q_lo0 + pchunk * a.probe_chunk;
+        m.q_hi = m.q_lo + a.probe_chunk < q_hi0 ? m.q_lo + a.probe_chunk : q_hi0;
+        m.p = p;
+        m.piece = static_cast<int32_t>(piece);
+        m.sbits = HASH_SPLIT ? split : 0;
+        return m;
+    };
     if (threadIdx.x == 0) {
         s_q = 0;
         s_next = static_cast<int64_t>(atomicAdd(a.queue, 1u));
+        if (s_next < total_items && s_next < a.max_items) s_nxt = load_meta(s_next);
     }
     if (threadIdx.x < OUT_SLOTS) s_cslot[threadIdx.x] = ~0ull;
 
@@ -593,48 +647,21 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         __syncthreads();
         if (threadIdx.x == 0) {
             s_item = s_next;
+            s_cur = s_nxt;
             s_next = static_cast<int64_t>(atomicAdd(a.queue, 1u));  // claim the next item early
         }
         __syncthreads();
         const int64_t item = s_item;
         if (item >= total_items || item >= a.max_items) break;
-        // first link of the next item's metadata chain, used at the probe start
-        int next_p = -1;
-        if (threadIdx.x == 0 && s_next < total_items && s_next < a.max_items) next_p = a.item_part[s_next];
-        const int p = a.item_part[item];
-        const int64_t local = item - a.item_off[p];
-        const int32_t split = a.split[p];
-        const int64_t S = HASH_SPLIT ? (1ll << split) : split;
-        const int64_t piece = local % S;
-        const int64_t pchunk = local / S;
-        const int sbits = HASH_SPLIT ? split : 0;
-        int dbits = a.digit_bits;
-        int64_t b_at = static_cast<int64_t>(p) * a.b_items, p_at = static_cast<int64_t>(p) * a.p_items;
-        int32_t b_n = a.b_items, p_n = a.p_items;
-        if constexpr (BATCH) {
-            const PartRef r = a.parts[p];
-            b_at = r.b_at;
-            p_at = r.p_at;
-            b_n = r.b_items;
-            p_n = r.p_items;
-            dbits = r.digit_bits;
-            jout = a.outs[r.job];
-        }
+        const int p = s_cur.p;
+        const int64_t piece = s_cur.piece;
+        const int sbits = s_cur.sbits;
+        const int dbits = s_cur.dbits;
+        const int64_t b_lo = s_cur.b_lo, b_hi = s_cur.b_hi;
+        const int64_t q_lo = s_cur.q_lo, q_hi = s_cur.q_hi;
+        if constexpr (BATCH) jout = s_cur.jout;
         const int skip = dbits + sbits;
         const int piece_shift = 32 - (sbits > 0 ? sbits : 1);
-
-        const int64_t b_lo0 = a.build_off[b_at];
-        const int64_t b_hi0 = a.build_off[b_at + b_n];
-        int64_t b_lo = b_lo0, b_hi = b_hi0;
-        if (!HASH_SPLIT) {
-            b_lo = b_lo0 + piece * a.position_chunk;
-            b_hi = b_lo + a.position_chunk < b_hi0 ? b_lo + a.position_chunk : b_hi0;
-            if (b_lo > b_hi) b_lo = b_hi;
-        }
-        const int64_t q_lo0 = a.probe_off[p_at];
-        const int64_t q_hi0 = a.probe_off[p_at + p_n];
-        const int64_t q_lo = q_lo0 + pchunk * a.probe_chunk;
-        const int64_t q_hi = q_lo + a.probe_chunk < q_hi0 ? q_lo + a.probe_chunk : q_hi0;
 
         // a CTA's first item: its build range was not prefetched during an
         // earlier probe phase
@@ -792,17 +819,12 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         // for COMPACT tables: their fingerprint checks re-read build tuples
         // and the prefetched ranges were evicted before use (0.83 GB more
         // DRAM reads at 2^27 x 2^27, no time gained).
-        if (TABLE != TABLE_COMPACT && threadIdx.x == 0 && next_p >= 0 && next_p != p) {
-            int64_t nb_at = static_cast<int64_t>(next_p) * a.b_items;
-            int32_t nb_n = a.b_items;
-            if constexpr (BATCH) {
-                nb_at = a.parts[next_p].b_at;
-                nb_n = a.parts[next_p].b_items;
+        if (threadIdx.x == 0 && s_next < total_items && s_next < a.max_items) {
+            s_nxt = load_meta(s_next);
+            if (TABLE != TABLE_COMPACT && s_nxt.p != p && s_nxt.b_hi > s_nxt.b_lo) {
+                const int64_t nbytes = (s_nxt.b_hi - s_nxt.b_lo) * TV::WORDS * 4;
+                prefetch_l2(a.build_tuples + s_nxt.b_lo * TV::WORDS, nbytes < (1 << 20) ? nbytes : (1 << 20));
             }
-            const int64_t nb_lo = a.build_off[nb_at];
-            const int64_t nb_hi = a.build_off[nb_at + nb_n];
-            const int64_t nbytes = (nb_hi - nb_lo) * TV::WORDS * 4;
-            prefetch_l2(a.build_tuples + nb_lo * TV::WORDS, nbytes < (1 << 20) ? nbytes : (1 << 20));
         }
 
         // ---- probe: warps run independently; loads run one step ahead ----
