@@ -292,7 +292,6 @@ __device__ __forceinline__ void walk_exact4(uint32_t& at, uint32_t& end, uint32_
                                             uint32_t lim)
 {
     asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 e, t;\n\t"
-                 "mov.b32 e, 0;\n\t"
                  "setp.lt.u32 p, %0, %1;\n\t"
                  "@p ld.shared.u32 e, [%0];\n\t"
                  "xor.b32 t, e, %4;\n\t"
@@ -312,8 +311,6 @@ __device__ __forceinline__ void walk_exact8(uint32_t& at, uint32_t& end, uint32_
                                             uint32_t lim, uint32_t klo)
 {
     asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 lo, e, t;\n\t"
-                 "mov.b32 lo, 0;\n\t"
-                 "mov.b32 e, 0;\n\t"
                  "setp.lt.u32 p, %0, %1;\n\t"
                  "@p ld.shared.v2.u32 {lo, e}, [%0];\n\t"
                  "xor.b32 t, e, %4;\n\t"
@@ -332,8 +329,6 @@ __device__ __forceinline__ void walk_exact8(uint32_t& at, uint32_t& end, uint32_
 __device__ __forceinline__ void walk_bucket8(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t k)
 {
     asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 ek, er;\n\t"
-                 "mov.b32 ek, 0;\n\t"
-                 "mov.b32 er, 0;\n\t"
                  "setp.lt.u32 p, %0, %1;\n\t"
                  "@p ld.shared.v2.u32 {ek, er}, [%0];\n\t"
                  "setp.eq.and.u32 q, ek, %4, p;\n\t"
@@ -443,7 +438,7 @@ struct JoinSmem {
     __host__ __device__ static size_t table_bytes(int cap, int nb_log2)
     {
         size_t t = entries_bytes(cap);
-        if (TABLE != TABLE_OPEN) t += ((static_cast<size_t>(1) << nb_log2) / 2) * 4;
+        if (TABLE != TABLE_OPEN) t += ((static_cast<size_t>(1) << nb_log2) / 2 + 1) * 4;
         return (t + 127) & ~size_t(127);
     }
     // dynamic shared memory of a join CTA: the table alone (matches go
@@ -613,16 +608,29 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
         q0 = __shfl_sync(0xffffffffu, q0, 0);
         if (!write_out) return;  // count only
         const uint32_t ch0 = q0 / OUT_CHUNK, ch1 = (q0 + n - 1) / OUT_CHUNK;
-        long long b0 = 0, b1 = 0;
-        if (lane == 0) b0 = chunk_base(ch0, q0 % OUT_CHUNK == 0);
-        if (lane == 1 && ch1 != ch0) b1 = chunk_base(ch1, true);  // its first position is ours
-        b0 = __shfl_sync(0xffffffffu, b0, 0);
-        b1 = __shfl_sync(0xffffffffu, b1, 1);
+        const bool first = q0 % OUT_CHUNK == 0;
+        if (first || ch1 != ch0) {  // rare: the step holds a chunk's first position and reserves it
+            if (lane == 0 && first) chunk_base(ch0, true);
+            if (lane == 1 && ch1 != ch0) chunk_base(ch1, true);
+            __syncwarp();
+        }
+        // every lane reads the bases (one broadcast load): no divergent lane
+        const long long b0 = chunk_base(ch0, false);
+        const long long b1 = ch1 != ch0 ? chunk_base(ch1, false) : 0;
         // entries [0, n0) go to chunk ch0 from position p0, the rest to ch1
         const int n0 = ch1 == ch0 ? n : static_cast<int>(ch1 * OUT_CHUNK - q0);
         const long long p0 = b0 + static_cast<long long>(q0 % OUT_CHUNK);
         const long long p1 = b1 - n0;
-        if (b0 >= 0 && p0 + n0 <= a.capacity && (n0 == n || (b1 >= 0 && b1 + (n - n0) <= a.capacity))) {
+        if (n0 == n && b0 >= 0 && p0 + n <= a.capacity) {  // one chunk: the common case
+            int32_t* ob = a.out_build + p0;
+            int32_t* op = a.out_probe + p0;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (emit[u]) {
+                    st_stream(ob + off[u], static_cast<int32_t>(brow[u]), stream_pol);
+                    st_stream(op + off[u], rp[u], stream_pol);
+                }
+        } else if (b0 >= 0 && p0 + n0 <= a.capacity && (n0 == n || (b1 >= 0 && b1 + (n - n0) <= a.capacity))) {
 #pragma unroll
             for (int u = 0; u < U; ++u)
                 if (emit[u]) {
@@ -701,7 +709,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             skip_item = true;
             __syncthreads();
         } else if constexpr (TABLE != TABLE_OPEN) {
-            for (int i = threadIdx.x; i < NB / 2; i += THREADS) ends[i] = 0u;
+            // bucket directory: 16-bit counts of bucket b at index b + 1; after
+            // the scan and the place pass index b holds the start of bucket b
+            // and index b + 1 its end
+            for (int i = threadIdx.x; i <= NB / 2; i += THREADS) ends[i] = 0u;
             if (threadIdx.x == 0) s_nbuild = 0;
             __syncthreads();
             // pass 1: count per bucket; the next batch of loads is issued
@@ -736,7 +747,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 #pragma unroll
                     for (int u = 0; u < JOIN_BU; ++u) {
                         if (r[u] >= 0 && in_piece(h[u])) {
-                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t b = bucket_of(h[u]) + 1u;
                             atomicAdd(&ends[b >> 1], (b & 1u) ? 0x10000u : 1u);
                             ++mine;
                         }
@@ -750,7 +761,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                 if (threadIdx.x == 0) raise_status(a.status, ST_OVERFLOW);
                 skip_item = true;
             } else {
-                scan_u16_pairs<THREADS>(ends, NB / 2, s_warp);
+                scan_u16_pairs<THREADS>(ends, NB / 2 + 1, s_warp);
                 // pass 2: place
                 const uint32_t* bt = a.build_tuples + b_lo * TV::WORDS;
                 const uint32_t bn = static_cast<uint32_t>(b_hi - b_lo);
@@ -767,7 +778,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 #pragma unroll
                     for (int u = 0; u < JOIN_BU; ++u) {
                         if (r[u] >= 0 && in_piece(h[u])) {
-                            const uint32_t b = bucket_of(h[u]);
+                            const uint32_t b = bucket_of(h[u]) + 1u;
                             const uint32_t old = atomicAdd(&ends[b >> 1], (b & 1u) ? 0x10000u : 1u);
                             const int pos = static_cast<int>((b & 1u) ? (old >> 16) : (old & 0xffffu));
                             if constexpr (TABLE == TABLE_COMPACT)
@@ -938,9 +949,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                 };
                 auto start = [&](int u, int& at_u, int& end_u, uint32_t& sl_u) {
                     if constexpr (TABLE != TABLE_OPEN) {
+                        const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
                         const uint32_t b = bucket_of(h[u]);
-                        end_u = static_cast<int>((ends[b >> 1] >> ((b & 1u) * 16)) & 0xffffu);
-                        at_u = b == 0 ? 0 : static_cast<int>((ends[(b - 1) >> 1] >> (((b - 1) & 1u) * 16)) & 0xffffu);
+                        at_u = e16[b];
+                        end_u = e16[b + 1];
                     } else {
                         sl_u = slot_of(h[u]);
                     }
@@ -961,11 +973,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                         live[u] = r[u] >= 0 && in_piece(h[u]);
                         at[u] = end[u] = 0;
                         if (live[u]) {
+                            const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
                             const uint32_t b = bucket_of(h[u]);
-                            const uint32_t wb = ends[b >> 1];
-                            const uint32_t wa = b == 0 ? 0u : ends[(b - 1) >> 1];
-                            end[u] = static_cast<int>((wb >> ((b & 1u) * 16)) & 0xffffu);
-                            at[u] = b == 0 ? 0 : static_cast<int>((wa >> (((b - 1) & 1u) * 16)) & 0xffffu);
+                            at[u] = e16[b];
+                            end[u] = e16[b + 1];
                             live[u] = at[u] < end[u];
                         }
                     }
@@ -1025,13 +1036,12 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                     for (int u = 0; u < U; ++u) {
                         raw[u] = 0u;
                         hit[u] = 0u;
-                        fqs[u] = xfinger_of(h[u]) << a.row_bits;
+                        fqs[u] = (h[u] >> a.nb_log2) << a.row_bits;  // xfinger_of(h) << R
                         const bool ok = r[u] >= 0 && in_piece(h[u]);
                         const uint32_t b = bucket_of(h[u]);
-                        const uint32_t e_hi = e16[b];
-                        const uint32_t e_lo = e16[(b - 1u) & nb_mask];
-                        end[u] = tb + (ok ? e_hi : 0u) * EB;
-                        at[u] = tb + ((ok && b != 0u) ? e_lo : 0u) * EB;
+                        const uint32_t e_lo = e16[b], e_hi = e16[b + 1];
+                        at[u] = tb + e_lo * EB;
+                        end[u] = ok ? tb + e_hi * EB : at[u];  // empty unless the tuple is live
                     }
                     for (;;) {
                         bool more = false;
@@ -1065,10 +1075,9 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             hit[u] = 0u;
                             const bool ok = r[u] >= 0 && in_piece(h[u]);
                             const uint32_t b = bucket_of(h[u]);
-                            const uint32_t e_hi = e16[b];
-                            const uint32_t e_lo = e16[(b - 1u) & nb_mask];
-                            end[u] = tb + (ok ? e_hi : 0u) * 8u;
-                            at[u] = tb + ((ok && b != 0u) ? e_lo : 0u) * 8u;
+                            const uint32_t e_lo = e16[b], e_hi = e16[b + 1];
+                            at[u] = tb + e_lo * 8u;
+                            end[u] = ok ? tb + e_hi * 8u : at[u];
                         }
                         for (;;) {
                             bool more = false;
@@ -1093,10 +1102,9 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             brow[u] = 0;
                             const bool ok = r[u] >= 0 && in_piece(h[u]);
                             const uint32_t b = bucket_of(h[u]);
-                            const int e_hi = e16[b];
-                            const int e_lo = e16[(b - 1u) & nb_mask];
+                            const int e_lo = e16[b], e_hi = e16[b + 1];
+                            at[u] = ok ? e_lo : 0;
                             end[u] = ok ? e_hi : 0;
-                            at[u] = (ok && b != 0u) ? e_lo : 0;
                         }
                         for (;;) {
                             bool more = false;
