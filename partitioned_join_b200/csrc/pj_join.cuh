@@ -283,62 +283,66 @@ template <> struct ExactEntry<int64_t> {
 // the cursor test, the skipped load and the updates are all predicated
 // instructions.  at / end: shared-window byte addresses of the tuple's
 // cursor and of its bucket's end; a lane whose cursor has reached the end
-// skips the load (no wavefront, no bank conflict).  On a match raw takes
-// the entry's row word, hit becomes 1 and end = at, so the walk stops.
+// skips the load (no wavefront, no bank conflict).  A match sets end = at,
+// so the walk stops with at = end + the entry size: afterwards at > end
+// marks a match, whose row word is the 4 bytes below at (walk_row).
 //
 // 4-byte EXACT entries: e matches when (e ^ fqs) < lim, i.e. its bits above
 // the row bits equal the tuple's tag (fqs = tag << R, lim = 1 << R).
-__device__ __forceinline__ void walk_exact4(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t fqs,
-                                            uint32_t lim)
+__device__ __forceinline__ void walk_exact4(uint32_t& at, uint32_t& end, uint32_t fqs, uint32_t lim)
 {
     asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 e, t;\n\t"
                  "setp.lt.u32 p, %0, %1;\n\t"
                  "@p ld.shared.u32 e, [%0];\n\t"
-                 "xor.b32 t, e, %4;\n\t"
-                 "setp.lt.and.u32 q, t, %5, p;\n\t"
-                 "@q mov.b32 %2, e;\n\t"
+                 "xor.b32 t, e, %2;\n\t"
+                 "setp.lt.and.u32 q, t, %3, p;\n\t"
                  "@q mov.b32 %1, %0;\n\t"
-                 "@q mov.b32 %3, 1;\n\t"
                  "@p add.u32 %0, %0, 4;\n\t"
                  "}"
-                 : "+r"(at), "+r"(end), "+r"(raw), "+r"(hit)
+                 : "+r"(at), "+r"(end)
                  : "r"(fqs), "r"(lim));
 }
 
 // 8-byte EXACT entries {key low word, tag << R | row}: the low word must
 // equal the tuple's too.
-__device__ __forceinline__ void walk_exact8(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t fqs,
-                                            uint32_t lim, uint32_t klo)
+__device__ __forceinline__ void walk_exact8(uint32_t& at, uint32_t& end, uint32_t fqs, uint32_t lim, uint32_t klo)
 {
     asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 lo, e, t;\n\t"
                  "setp.lt.u32 p, %0, %1;\n\t"
                  "@p ld.shared.v2.u32 {lo, e}, [%0];\n\t"
-                 "xor.b32 t, e, %4;\n\t"
-                 "setp.lt.and.u32 q, t, %5, p;\n\t"
-                 "setp.eq.and.u32 q, lo, %6, q;\n\t"
-                 "@q mov.b32 %2, e;\n\t"
+                 "xor.b32 t, e, %2;\n\t"
+                 "setp.lt.and.u32 q, t, %3, p;\n\t"
+                 "setp.eq.and.u32 q, lo, %4, q;\n\t"
                  "@q mov.b32 %1, %0;\n\t"
-                 "@q mov.b32 %3, 1;\n\t"
                  "@p add.u32 %0, %0, 8;\n\t"
                  "}"
-                 : "+r"(at), "+r"(end), "+r"(raw), "+r"(hit)
+                 : "+r"(at), "+r"(end)
                  : "r"(fqs), "r"(lim), "r"(klo));
 }
 
 // 8-byte BUCKET entries {key, row} of 4-byte keys: a match is key == k.
-__device__ __forceinline__ void walk_bucket8(uint32_t& at, uint32_t& end, uint32_t& raw, uint32_t& hit, uint32_t k)
+__device__ __forceinline__ void walk_bucket8(uint32_t& at, uint32_t& end, uint32_t k)
 {
-    asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 ek, er;\n\t"
+    asm volatile("{\n\t.reg .pred p, q;\n\t.reg .b32 ek;\n\t"
                  "setp.lt.u32 p, %0, %1;\n\t"
-                 "@p ld.shared.v2.u32 {ek, er}, [%0];\n\t"
-                 "setp.eq.and.u32 q, ek, %4, p;\n\t"
-                 "@q mov.b32 %2, er;\n\t"
+                 "@p ld.shared.u32 ek, [%0];\n\t"
+                 "setp.eq.and.u32 q, ek, %2, p;\n\t"
                  "@q mov.b32 %1, %0;\n\t"
-                 "@q mov.b32 %3, 1;\n\t"
                  "@p add.u32 %0, %0, 8;\n\t"
                  "}"
-                 : "+r"(at), "+r"(end), "+r"(raw), "+r"(hit)
+                 : "+r"(at), "+r"(end)
                  : "r"(k));
+}
+
+// After a walk: whether the cursor stopped on a match, and that entry's row
+// word (its last 4 bytes, just below the cursor); 0 without a match.
+__device__ __forceinline__ uint32_t walk_row(uint32_t at, uint32_t end)
+{
+    uint32_t v = 0u;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.gt.u32 p, %1, %2;\n\t@p ld.shared.u32 %0, [%3];\n\t}"
+                 : "+r"(v)
+                 : "r"(at), "r"(end), "r"(at - 4u));
+    return v;
 }
 
 // Entry of a BUCKET table.
@@ -1030,12 +1034,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                     const uint32_t tb = static_cast<uint32_t>(__cvta_generic_to_shared(table));
                     const uint32_t lim = 1u << a.row_bits;
                     bool emit[U];
-                    uint32_t brow[U], raw[U], hit[U], fqs[U], at[U], end[U];
+                    uint32_t brow[U], fqs[U], at[U], end[U];
                     const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        raw[u] = 0u;
-                        hit[u] = 0u;
                         fqs[u] = (h[u] >> a.nb_log2) << a.row_bits;  // xfinger_of(h) << R
                         const bool ok = r[u] >= 0 && in_piece(h[u]);
                         const uint32_t b = bucket_of(h[u]);
@@ -1048,17 +1050,17 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
                             if constexpr (EB == 4)
-                                walk_exact4(at[u], end[u], raw[u], hit[u], fqs[u], lim);
+                                walk_exact4(at[u], end[u], fqs[u], lim);
                             else
-                                walk_exact8(at[u], end[u], raw[u], hit[u], fqs[u], lim, ExactEntry<K>::key_lo(k[u]));
+                                walk_exact8(at[u], end[u], fqs[u], lim, ExactEntry<K>::key_lo(k[u]));
                             more = more || at[u] < end[u];
                         }
                         if (!__any_sync(0xffffffffu, more)) break;
                     }
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        emit[u] = hit[u] != 0u;
-                        brow[u] = raw[u] & x_rmask;
+                        emit[u] = at[u] > end[u];  // a match stopped the cursor past its end
+                        brow[u] = walk_row(at[u], end[u]) & x_rmask;
                     }
                     append_direct(emit, brow, r);
                 } else if constexpr (UNIQUE && TABLE == TABLE_BUCKET) {
@@ -1067,12 +1069,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                     if constexpr (Entry<K>::BYTES == 8) {
                         const uint32_t tb = static_cast<uint32_t>(__cvta_generic_to_shared(table));
                         bool emit[U];
-                        uint32_t brow[U], hit[U], at[U], end[U];
+                        uint32_t brow[U], at[U], end[U];
                         const uint16_t* e16 = reinterpret_cast<const uint16_t*>(ends);
 #pragma unroll
                         for (int u = 0; u < U; ++u) {
-                            brow[u] = 0u;
-                            hit[u] = 0u;
                             const bool ok = r[u] >= 0 && in_piece(h[u]);
                             const uint32_t b = bucket_of(h[u]);
                             const uint32_t e_lo = e16[b], e_hi = e16[b + 1];
@@ -1083,13 +1083,16 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
                             bool more = false;
 #pragma unroll
                             for (int u = 0; u < U; ++u) {
-                                walk_bucket8(at[u], end[u], brow[u], hit[u], static_cast<uint32_t>(k[u]));
+                                walk_bucket8(at[u], end[u], static_cast<uint32_t>(k[u]));
                                 more = more || at[u] < end[u];
                             }
                             if (!__any_sync(0xffffffffu, more)) break;
                         }
 #pragma unroll
-                        for (int u = 0; u < U; ++u) emit[u] = hit[u] != 0u;
+                        for (int u = 0; u < U; ++u) {
+                            emit[u] = at[u] > end[u];
+                            brow[u] = walk_row(at[u], end[u]);
+                        }
                         append_direct(emit, brow, r);
                     } else {  // 12-byte entries {key, row} of 8-byte keys
                         bool emit[U];
