@@ -188,6 +188,30 @@ __device__ __forceinline__ void st_stream(int32_t* p, int32_t v, uint64_t pol)
     asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
 }
 
+// Predicated forms: lanes with pred == false skip the access.  One
+// predicated instruction each, so the hot loops carry no divergent branch
+// around them.
+__device__ __forceinline__ void st_stream_if(int32_t* p, int32_t v, bool pred, uint64_t pol)
+{
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.L2::cache_hint.b32 [%0], %1, %3;\n\t}"
+                 ::"l"(p), "r"(v), "r"(static_cast<uint32_t>(pred)), "l"(pol)
+                 : "memory");
+}
+// v keeps its value where pred is false
+__device__ __forceinline__ void ld_stream_if(uint2& v, const uint2* p, bool pred, uint64_t pol)
+{
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t"
+                 "@q ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %4;\n\t}"
+                 : "+r"(v.x), "+r"(v.y)
+                 : "l"(p), "r"(static_cast<uint32_t>(pred)), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_if(uint4& v, const uint4* p, bool pred, uint64_t pol)
+{
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t"
+                 "@q ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %6;\n\t}"
+                 : "+r"(v.x), "+r"(v.y), "+r"(v.z), "+r"(v.w)
+                 : "l"(p), "r"(static_cast<uint32_t>(pred)), "l"(pol));
+}
 // ---------------------------------------------------------------------------
 // Tuple access: a probe/build tuple gives (hash, comparable key, row).
 // 4-byte keys: the stored word 0 is murmur(key), a bijection, so the hash is
@@ -208,6 +232,16 @@ template <> struct TupleView<int32_t> {
                                                        int32_t& row, uint64_t pol)
     {
         const uint2 v = ld_stream(reinterpret_cast<const uint2*>(base) + i, pol);
+        h = v.x;
+        key = v.x;
+        row = static_cast<int32_t>(v.y);
+    }
+    // row = -1 where pred is false
+    __device__ __forceinline__ static void load_stream_if(const uint32_t* base, int64_t i, bool pred, uint32_t& h,
+                                                          Cmp& key, int32_t& row, uint64_t pol)
+    {
+        uint2 v = make_uint2(0u, 0xffffffffu);
+        ld_stream_if(v, reinterpret_cast<const uint2*>(base) + i, pred, pol);
         h = v.x;
         key = v.x;
         row = static_cast<int32_t>(v.y);
@@ -234,6 +268,15 @@ template <> struct TupleView<int64_t> {
                                                        int32_t& row, uint64_t pol)
     {
         const uint4 v = ld_stream(reinterpret_cast<const uint4*>(base) + i, pol);
+        key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
+        h = v.z;
+        row = static_cast<int32_t>(v.w);
+    }
+    __device__ __forceinline__ static void load_stream_if(const uint32_t* base, int64_t i, bool pred, uint32_t& h,
+                                                          Cmp& key, int32_t& row, uint64_t pol)
+    {
+        uint4 v = make_uint4(0u, 0u, 0u, 0xffffffffu);
+        ld_stream_if(v, reinterpret_cast<const uint4*>(base) + i, pred, pol);
         key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
         h = v.z;
         row = static_cast<int32_t>(v.w);
@@ -629,11 +672,10 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
             int32_t* ob = a.out_build + p0;
             int32_t* op = a.out_probe + p0;
 #pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (emit[u]) {
-                    st_stream(ob + off[u], static_cast<int32_t>(brow[u]), stream_pol);
-                    st_stream(op + off[u], rp[u], stream_pol);
-                }
+            for (int u = 0; u < U; ++u) {
+                st_stream_if(ob + off[u], static_cast<int32_t>(brow[u]), emit[u], stream_pol);
+                st_stream_if(op + off[u], rp[u], emit[u], stream_pol);
+            }
         } else if (b0 >= 0 && p0 + n0 <= a.capacity && (n0 == n || (b1 >= 0 && b1 + (n - n0) <= a.capacity))) {
 #pragma unroll
             for (int u = 0; u < U; ++u)
@@ -861,8 +903,7 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const uint32_t i = s0 + u * 32 + lane;
-                    nr[u] = -1;
-                    if (i < qn) TV::load_stream(pbase, i, nh[u], nk[u], nr[u], stream_pol);
+                    TV::load_stream_if(pbase, i, i < qn, nh[u], nk[u], nr[u], stream_pol);
                 }
             };
             uint32_t s0 = claim();
