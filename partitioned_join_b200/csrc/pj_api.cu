@@ -706,7 +706,8 @@ pj_status launch_join_t(const JoinArgs& a, cudaStream_t st)
     kern<<<grid, JN_THREADS, smem, st>>>(a);
     PJ_CUDA(cudaGetLastError());
     // fix-up: dense output and the true count
-    join_fixup_plan_kernel<<<1, MAX_FIXUP_CTAS, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.base_count, a.capacity,
+    const int fix_threads = std::min(MAX_FIXUP_CTAS, (grid + 31) / 32 * 32);
+    join_fixup_plan_kernel<<<1, fix_threads, 0, st>>>(a.cta_q, a.cta_last, grid, a.count, a.base_count, a.capacity,
                                                a.out_build != nullptr ? 1 : 0, a.seg, a.status);
     PJ_CUDA(cudaGetLastError());
     if (a.out_build != nullptr) {

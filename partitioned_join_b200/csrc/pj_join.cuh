@@ -1253,6 +1253,35 @@ __global__ void __launch_bounds__(THREADS, 1) join_kernel(JoinArgs a)
 // hole (start, prefix) pairs, then mover (start, prefix) pairs.
 constexpr int MAX_FIXUP_CTAS = 1024;  // join CTAs one fix-up plan covers: one thread (and gap) each
 
+// Exclusive prefix over the block of one value per thread; the block's
+// total goes to *total (every thread).  Contains two barriers.
+__device__ __forceinline__ long long block_excl_scan(long long v, long long* s_w, long long* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    long long incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    long long before = 0, all = 0;
+    for (int w = 0; w < nw; ++w) {
+        before += w < warp ? s_w[w] : 0;
+        all += s_w[w];
+    }
+    *total = all;
+    __syncthreads();  // s_w is free again
+    return before + incl - v;
+}
+
+// One block of at least n_cta threads (a multiple of 32).  Thread c takes
+// CTA c's gap (the unused tail of its last chunk); the gaps are ranked by
+// start, and thread g then works out the hole below the true total that
+// gap g leaves and the stretch of entries at or above the total that ends
+// at it; block scans number both lists.  The stretch after the last gap is
+// thread 0's.
 __global__ void __launch_bounds__(MAX_FIXUP_CTAS) join_fixup_plan_kernel(const int64_t* __restrict__ cta_q,
                                                                const int64_t* __restrict__ cta_last, int32_t n_cta,
                                                                unsigned long long* count,
@@ -1261,82 +1290,83 @@ __global__ void __launch_bounds__(MAX_FIXUP_CTAS) join_fixup_plan_kernel(const i
                                                                int32_t write_out, int64_t* __restrict__ seg,
                                                                uint32_t* __restrict__ status)
 {
-    __shared__ long long s_sum;
-    __shared__ long long g_start[MAX_FIXUP_CTAS], g_len[MAX_FIXUP_CTAS];
-    __shared__ int s_ng;
+    __shared__ long long g_at[MAX_FIXUP_CTAS];                        // gap start by CTA (-1: none)
+    __shared__ long long g_start[MAX_FIXUP_CTAS], g_end[MAX_FIXUP_CTAS];  // gaps by rank
+    __shared__ long long s_w[32];
+    const int t = threadIdx.x;
     if (n_cta > static_cast<int>(blockDim.x)) {  // gaps of CTAs past the block would stay unfilled
-        if (threadIdx.x == 0) raise_status(status, ST_INTERNAL);
+        if (t == 0) raise_status(status, ST_INTERNAL);
         return;
     }
-    if (threadIdx.x == 0) {
-        s_sum = 0;
-        s_ng = 0;
-    }
-    __syncthreads();
-    long long mine = 0;
-    for (int c = threadIdx.x; c < n_cta; c += blockDim.x) mine += cta_q[c];
-    atomicAdd(reinterpret_cast<unsigned long long*>(&s_sum), static_cast<unsigned long long>(mine));
-    // gaps, placed at their rank by start (starts are distinct chunk positions)
-    long long my_start = -1, my_len = 0;
-    if (threadIdx.x < n_cta && write_out) {
-        const long long q = cta_q[threadIdx.x], rem = q % OUT_CHUNK;
-        if (q > 0 && rem != 0 && cta_last[threadIdx.x] >= 0) {
-            my_start = cta_last[threadIdx.x] + rem;
-            my_len = OUT_CHUNK - rem;
+    long long q = 0, gs = -1, ge = -1;
+    if (t < n_cta) {
+        q = cta_q[t];
+        const long long rem = q % OUT_CHUNK;
+        if (write_out && q > 0 && rem != 0 && cta_last[t] >= 0) {
+            gs = cta_last[t] + rem;
+            ge = cta_last[t] + OUT_CHUNK;
         }
     }
-    __syncthreads();
-    if (my_start >= 0) {
+    g_at[t] = gs;
+    long long sum, ng;
+    block_excl_scan(q, s_w, &sum);  // its barriers also publish g_at
+    const long long total = sum + (base_count ? static_cast<long long>(*base_count) : 0);
+    const long long reserved = static_cast<long long>(*count);
+    // rank by start: starts are distinct positions of distinct chunks
+    if (gs >= 0) {
         int rank = 0;
-        for (int c = 0; c < n_cta; ++c) {
-            const long long q = cta_q[c], rem = q % OUT_CHUNK;
-            if (q > 0 && rem != 0 && cta_last[c] >= 0 && cta_last[c] + rem < my_start) ++rank;
-        }
-        g_start[rank] = my_start;
-        g_len[rank] = my_len;
-        atomicAdd(&s_ng, 1);
+        for (int c = 0; c < n_cta; ++c) rank += (g_at[c] >= 0 && g_at[c] < gs) ? 1 : 0;
+        g_start[rank] = gs;
+        g_end[rank] = ge;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const long long total = s_sum + (base_count ? static_cast<long long>(*base_count) : 0);
-        const long long reserved = static_cast<long long>(*count);
+    block_excl_scan(gs >= 0 ? 1 : 0, s_w, &ng);  // and publish the ranked gaps
+    const bool lists = write_out && total <= capacity;
+    long long h_len = 0, m_lo = 0, m_len = 0, h_at = 0;
+    if (lists && t < ng) {
+        h_at = g_start[t];
+        const long long h_end = g_end[t];
+        if (h_at < total) h_len = (h_end < total ? h_end : total) - h_at;
+        // entries from the previous gap's end (or 0) up to this gap, at or above the total
+        const long long prev = t > 0 ? g_end[t - 1] : 0;
+        m_lo = prev > total ? prev : total;
+        const long long hi = h_at < reserved ? h_at : reserved;
+        m_len = hi > m_lo ? hi - m_lo : 0;
+    }
+    long long nh, hp, nm, mp;
+    const long long h_idx = block_excl_scan(h_len > 0 ? 1 : 0, s_w, &nh);
+    const long long h_pre = block_excl_scan(h_len, s_w, &hp);
+    const long long m_idx = block_excl_scan(m_len > 0 ? 1 : 0, s_w, &nm);
+    const long long m_pre = block_excl_scan(m_len, s_w, &mp);
+    int64_t* hole = seg + 4;
+    int64_t* mover = seg + 4 + 2 * (n_cta + 2);
+    if (h_len > 0) {
+        hole[2 * h_idx] = h_at;
+        hole[2 * h_idx + 1] = h_pre;
+    }
+    if (m_len > 0) {
+        mover[2 * m_idx] = m_lo;
+        mover[2 * m_idx + 1] = m_pre;
+    }
+    if (t == 0) {
         *count = static_cast<unsigned long long>(total);
-        int nh = 0, nm = 0;
         long long moves = 0;
-        if (write_out && total <= capacity) {
-            int64_t* hole = seg + 4;
-            int64_t* mover = seg + 4 + 2 * (n_cta + 2);
-            long long hp = 0, mp = 0, cur = total;
-            for (int g = 0; g < s_ng; ++g) {
-                const long long gs = g_start[g], ge = g_start[g] + g_len[g];
-                if (gs < total) {  // hole: the part of the gap below total
-                    hole[2 * nh] = gs;
-                    hole[2 * nh + 1] = hp;
-                    hp += (ge < total ? ge : total) - gs;
-                    ++nh;
-                }
-                if (ge <= cur) continue;
-                if (gs > cur) {  // valid entries between the previous gap and this one
-                    const long long e = gs < reserved ? gs : reserved;
-                    if (e > cur) {
-                        mover[2 * nm] = cur;
-                        mover[2 * nm + 1] = mp;
-                        mp += e - cur;
-                        ++nm;
-                    }
-                }
-                if (ge > cur) cur = ge;
-            }
-            if (cur < reserved) {
-                mover[2 * nm] = cur;
+        if (lists) {
+            // the entries after the last gap
+            const long long last = ng > 0 ? g_end[ng - 1] : 0;
+            const long long lo = last > total ? last : total;
+            if (reserved > lo) {
+                mover[2 * nm] = lo;
                 mover[2 * nm + 1] = mp;
-                mp += reserved - cur;
+                mp += reserved - lo;
                 ++nm;
             }
             if (hp != mp) raise_status(status, ST_INTERNAL);
             moves = hp < mp ? hp : mp;
-        } else if (write_out && total > capacity) {
+        } else if (write_out) {
             raise_status(status, ST_CAPACITY);
+            nh = nm = 0;
+        } else {
+            nh = nm = 0;
         }
         seg[0] = nh;
         seg[1] = nm;
