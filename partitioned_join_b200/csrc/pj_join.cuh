@@ -167,22 +167,6 @@ __device__ __forceinline__ uint64_t l2_evict_first_policy()
     return pol;
 }
 
-__device__ __forceinline__ uint2 ld_stream(const uint2* p, uint64_t pol)
-{
-    uint2 v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
-                 : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
-    return v;
-}
-
-__device__ __forceinline__ uint4 ld_stream(const uint4* p, uint64_t pol)
-{
-    uint4 v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
-    return v;
-}
-
 __device__ __forceinline__ void st_stream(int32_t* p, int32_t v, uint64_t pol)
 {
     asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
@@ -212,6 +196,7 @@ __device__ __forceinline__ void ld_stream_if(uint4& v, const uint4* p, bool pred
                  : "+r"(v.x), "+r"(v.y), "+r"(v.z), "+r"(v.w)
                  : "l"(p), "r"(static_cast<uint32_t>(pred)), "l"(pol));
 }
+
 // ---------------------------------------------------------------------------
 // Tuple access: a probe/build tuple gives (hash, comparable key, row).
 // 4-byte keys: the stored word 0 is murmur(key), a bijection, so the hash is
@@ -224,14 +209,6 @@ template <> struct TupleView<int32_t> {
     __device__ __forceinline__ static void load(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key, int32_t& row)
     {
         const uint2 v = __ldg(reinterpret_cast<const uint2*>(base) + i);
-        h = v.x;
-        key = v.x;
-        row = static_cast<int32_t>(v.y);
-    }
-    __device__ __forceinline__ static void load_stream(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key,
-                                                       int32_t& row, uint64_t pol)
-    {
-        const uint2 v = ld_stream(reinterpret_cast<const uint2*>(base) + i, pol);
         h = v.x;
         key = v.x;
         row = static_cast<int32_t>(v.y);
@@ -260,14 +237,6 @@ template <> struct TupleView<int64_t> {
     __device__ __forceinline__ static void load(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key, int32_t& row)
     {
         const uint4 v = __ldg(reinterpret_cast<const uint4*>(base) + i);
-        key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
-        h = v.z;
-        row = static_cast<int32_t>(v.w);
-    }
-    __device__ __forceinline__ static void load_stream(const uint32_t* base, int64_t i, uint32_t& h, Cmp& key,
-                                                       int32_t& row, uint64_t pol)
-    {
-        const uint4 v = ld_stream(reinterpret_cast<const uint4*>(base) + i, pol);
         key = (static_cast<unsigned long long>(v.y) << 32) | v.x;
         h = v.z;
         row = static_cast<int32_t>(v.w);
