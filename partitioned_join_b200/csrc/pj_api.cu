@@ -28,7 +28,8 @@ constexpr int SC_V32 = 4, SC_V64 = 2;  // keys per thread per round (one 16-byte
 #ifndef PJ_JOIN_THREADS
 // 24 warps of up to 85 registers: the 1024-thread form (64 registers) spilled
 // in the probe loop; 2^27 x 2^27 int32 join 2.43 -> 2.37 ms, 2^26 x 2^28
-// int64 4.37 -> 3.73 ms (512, 640, 896 threads all measured slower)
+// int64 4.37 -> 3.73 ms (512, 640, 896 threads all measured slower; 832
+// threads: int32 0.997 -> 1.007 ms, int64 1.95 -> 1.93 ms)
 constexpr int JN_THREADS = 768;
 #else
 constexpr int JN_THREADS = PJ_JOIN_THREADS;
