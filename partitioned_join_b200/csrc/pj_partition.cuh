@@ -819,8 +819,17 @@ __global__ void __launch_bounds__(HIST_THREADS) hist_seg_kernel(const SegItem* _
     int64_t s_lo = it.lo + part * per;
     const int64_t s_hi = s_lo + per < it.hi ? s_lo + per : it.hi;
     if (s_lo > s_hi) s_lo = s_hi;
-    for (int64_t i = s_lo + threadIdx.x; i < s_hi; i += HIST_THREADS)
-        atomicAdd(&cnt[(hash_key(keys[i]) >> it.f.shift) & it.f.mask], 1u);
+    // SEG_UNROLL independent loads in flight per thread, then their counts
+    constexpr int SEG_UNROLL = 8;
+    int64_t i = s_lo + threadIdx.x;
+    for (; i + (SEG_UNROLL - 1) * HIST_THREADS < s_hi; i += SEG_UNROLL * HIST_THREADS) {
+        K k[SEG_UNROLL];
+#pragma unroll
+        for (int u = 0; u < SEG_UNROLL; ++u) k[u] = __ldg(keys + i + u * HIST_THREADS);
+#pragma unroll
+        for (int u = 0; u < SEG_UNROLL; ++u) atomicAdd(&cnt[(hash_key(k[u]) >> it.f.shift) & it.f.mask], 1u);
+    }
+    for (; i < s_hi; i += HIST_THREADS) atomicAdd(&cnt[(hash_key(keys[i]) >> it.f.shift) & it.f.mask], 1u);
     __syncthreads();
     for (int p = threadIdx.x; p < it.P; p += HIST_THREADS) {
         const uint32_t c = cnt[p];
