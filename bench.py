@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--cfg4-max-log2-build", type=int, default=28)
     ap.add_argument("--cfg4-max-log2-probe", type=int, default=29)
     ap.add_argument("--batch", type=int, default=512, help="cfg5: joins in the batch")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="cfg5: only the batch in its default configuration (for launch lists)")
     ap.add_argument("--zipf", type=float, default=1.0, help="cfg3: Zipf exponent of the probe keys")
     ap.add_argument("--log2-build", type=int, default=None)
     ap.add_argument("--log2-probe", type=int, default=None)
@@ -657,6 +659,18 @@ def run_batch(args, rank, world, local, emit=True):
                if not verify_pairs_device(b, p, brs[i], prs[i], cnts[i], expected[i])["ok"]]
         return {"joins_checked": len(pairs), "pairs_checked": int(sum(cnts)), "failed_joins": bad[:8],
                 "ok": not bad}
+
+    if args.batch_only:
+        bj = api.BatchJoiner(pairs)
+        ms = timed(bj.launch, max(1, args.steps))
+        bj.check()
+        ok = verify_all(bj.build_row, bj.probe_row, bj.count)
+        line = {"metric": "batch ms, default configuration (cfg5, batch only)", "value": ms, "unit": "ms",
+                "higher_is_better": False, "config": {"workload": f"{args.batch} int32 joins (cfg5)"},
+                "verified": ok}
+        if emit and rank == 0:
+            print(json.dumps(line), flush=True)
+        return line
 
     steps = max(1, min(args.steps, 5))
     plain_ms = timed(plain, steps)
